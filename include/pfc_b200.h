@@ -1,0 +1,133 @@
+/*
+ * pfc_b200.h — C ABI of the B200 spectral relaxation library (libpfc_b200.so).
+ *
+ * The reference (petenez/pfc, pfc-relax.c) has no library API: its hot path is
+ * the set of functions relax() calls between the host parser and FFTW-MPI.
+ * Each entry point below replaces one of those functions (cited per entry).
+ * Line numbers refer to demos/honey/pfc-relax.c, the copy the oracle is built
+ * from; src/pfc-relax.c lacks its line 499, so subtract 1 from lines >= 500 there.
+ *
+ * Conventions
+ *  - Plain C types only; the caller owns every host buffer it passes.
+ *  - The library owns device memory, one CUDA stream and its graphs per handle.
+ *    One handle per host thread; handles are independent (no global state).
+ *  - Real fields cross the boundary unpadded, y-major: value (x=i, y=j) of
+ *    component u is at fields[(u*Ny + j)*Nx + i] — the order of the .n files
+ *    (pfc-relax.c:748-755, 803-809).
+ *  - Return value: 0 = success; positive = the reference's fail() code for the
+ *    same condition (pfc-relax.c:242-411), e.g. 39 = NaN detected; negative =
+ *    a library error (PFCG_E*), with a message from pfcg_last_error().
+ */
+#ifndef PFC_B200_H
+#define PFC_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFCG_MAX_U 4 /* density fields per system */
+#define PFCG_MAX_W 4 /* modes per density field */
+
+/* error codes (library-side; positive codes are the reference's fail() codes) */
+#define PFCG_OK 0
+#define PFCG_NAN 39         /* pfc-relax.c:402-404, "Not a number value detected." */
+#define PFCG_EARG (-1)      /* invalid argument */
+#define PFCG_ECUDA (-2)     /* CUDA runtime error */
+#define PFCG_ESIZE (-3)     /* grid size not supported (see pfcg_size_supported) */
+#define PFCG_ENOMEM (-4)    /* device allocation failed */
+#define PFCG_ETIMEOUT (-5)  /* a bounded device-side wait ran out */
+#define PFCG_ENODEV (-6)    /* no CUDA device / not an sm_100 device */
+
+typedef enum { PFCG_FP32 = 0, PFCG_FP64 = 1 } pfcg_prec;
+
+/* Model parameters, stored the way pfc-relax.c's read_input leaves them in
+ * struct S (pfc-relax.c:34-120, 542-705):
+ *   nu2[u][w] = 1/(1/nu)^2 (:655), mu2[u][v] = 1/(1/mu)^2, or 0 when beta[u][v]
+ *   == 0 (:699-700). Matrices are read in their upper triangle (v >= u; v > u
+ *   for epsilon and mu2). c is the raw input value: 0 = nonconserved, any other
+ *   value = conserved (:930). */
+typedef struct pfcg_params {
+	int U;
+	int W[PFCG_MAX_U];
+	double c;
+	double sigma;
+	double dt;
+	double lambda[PFCG_MAX_U];
+	double delta[PFCG_MAX_U];
+	double alpha[PFCG_MAX_U][PFCG_MAX_U];
+	double beta[PFCG_MAX_U][PFCG_MAX_U];
+	double gamma[PFCG_MAX_U][PFCG_MAX_U];
+	double epsilon[PFCG_MAX_U][PFCG_MAX_U];
+	double mu2[PFCG_MAX_U][PFCG_MAX_U];
+	double nu2[PFCG_MAX_U][PFCG_MAX_W];
+	double omega[PFCG_MAX_U][PFCG_MAX_W];
+	double phi[PFCG_MAX_U][PFCG_MAX_W];
+} pfcg_params;
+
+typedef struct pfcg_handle pfcg_handle;
+
+/* 1 if an Nx x Ny grid is supported (both even, 8 <= N <= 8192, N = 2^a 3^b 5^c 7^d),
+ * else 0. The reference accepts any size through FFTW; sizes outside this set
+ * are rejected with PFCG_ESIZE instead of falling back to a CPU path. */
+int pfcg_size_supported(int Nx, int Ny);
+
+/* Creates a relaxation of U = p->U fields on an Nx x Ny grid with spacing dx, dy.
+ * Replaces initialize() minus read_data: allocate_data (:162-193), plan_FFTs
+ * (:196-239) and update_AB (:901-958). prec selects the FFT/pointwise precision;
+ * reductions, the k=0 (mean) mode and the box optimisation are FP64 in both. */
+int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg_prec prec, pfcg_handle** out);
+
+/* Uploads the real fields (U*Ny*Nx doubles, layout above) as the state at time
+ * t = 0. Replaces read_data (:729-764) filling m[u], plus the first spectral
+ * synchronisation step() does at t = 0 (:1179-1185). */
+int pfcg_upload(pfcg_handle* h, const double* fields);
+
+/* Downloads the current real fields (U*Ny*Nx doubles). Replaces the m[u] that
+ * write_data prints (:803-809). */
+int pfcg_download(pfcg_handle* h, double* fields);
+
+/* Sets the grid spacing and rebuilds the linear operators. Replaces update_AB
+ * (:901-958) after a change of s->dx, s->dy. */
+int pfcg_set_box(pfcg_handle* h, double dx, double dy);
+int pfcg_get_box(const pfcg_handle* h, double* dx, double* dy);
+
+/* Relaxation step counter t used for the every-100-steps resynchronisation of
+ * the spectral state (:1179-1185). pfcg_upload sets t = 0, pfcg_step advances it. */
+int pfcg_set_time(pfcg_handle* h, int t);
+int pfcg_get_time(const pfcg_handle* h, int* t);
+
+/* Advances nsteps semi-implicit (ETD1) steps. Replaces step() (:1134-1248)
+ * called nsteps times. Returns 39 if a NaN appeared in the field (the
+ * reference checks m[0][0] at :1176; this checks every point). */
+int pfcg_step(pfcg_handle* h, int nsteps);
+
+/* Computes <f> and <n_u> of the current state, and the free-energy density f(r)
+ * (Ny*Nx doubles) when f != NULL. Replaces evaluate() (:988-1131). The gradient
+ * coupling uses mu2 as intended; the reference reads nu2 there (:1020), which
+ * only matters when some beta[u][v] != 0 with u < v. */
+int pfcg_evaluate(pfcg_handle* h, double* fave, double* nave, double* f);
+
+/* One box-size optimisation. Replaces optimize() (:1251-1290): samples <f> at
+ * dx, dx -/+ d and dy -/+ d, moves to the parabola vertex with the change
+ * clamped to a quarter lattice constant, rebuilds the operators and adapts d.
+ * *d is the sampling step (in/out; relax() starts it at 1e-4, :1296). */
+int pfcg_optimize(pfcg_handle* h, int xopt, int yopt, double* d);
+
+/* The CUDA stream the handle launches on (a cudaStream_t), for timing. */
+int pfcg_stream(const pfcg_handle* h, void** stream);
+
+/* Number of kernel launches the handle has issued so far. */
+int pfcg_launch_count(const pfcg_handle* h, long long* count);
+
+/* Last error message of the handle (or of the last failed pfcg_create when h is NULL). */
+const char* pfcg_last_error(const pfcg_handle* h);
+
+void pfcg_destroy(pfcg_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
