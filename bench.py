@@ -1,0 +1,342 @@
+"""Benchmark of the spectral relaxation step (pfc-relax's hot path) on B200.
+
+Workload (default): the two-component lateral heterostructure at 4096 x 4096
+(U = 2, conserved dynamics, dt = 0.25, epsilon_01 smoothed-density coupling,
+4% lattice mismatch), seeded synthetic initial state of alternating 512-wide
+stripes plus noise. A step is one semi-implicit (ETD1) step of all fields:
+x-pass (c2r, nonlinear term, r2c along x) and y-pass (FFT along y, coupling
+and update, inverse FFT along y). The working set (spectral state + mixed
+workspace, 268 MB in FP32) is larger than L2 (126 MB), so no L2 flush is
+needed between timed steps.
+
+    python bench.py [--gpus N --steps K --warmup W] [--precision fp32|fp64]
+    python bench.py --impl reference   # the reference solver's CPU step
+
+Multi-GPU: one process per GPU (torchrun), each rank relaxes its own replica
+(independent seeds, no collective in the data path): weak scaling. The time is
+the max over ranks of the device-timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from pfc_b200 import lib, nfile, synth  # noqa: E402
+from pfc_b200 import params as P  # noqa: E402
+
+METRIC = "steps/s & time-to-relaxed at 4096² 2-comp, FP32/warm-start vs plain FP64 on 1 B200"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def workload(N: int, rank: int):
+    """Parameters, box and initial fields of the heterostructure workload."""
+    pd = P.hetero_2c(0.04)
+    dx = dy = 0.7
+    a0 = 7.2552
+    f = synth.stripes2(N, N, dx, dy, 512 if N >= 2048 else max(N // 8, 8), (0.3, -0.3), (0.3, 0.3),
+                       (a0, a0 * 1.04), 0.02, 1000 + rank)
+    return pd, dx, dy, f
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 8:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def traffic_from_profiles(kernel: str, workload_name: str):
+    """DRAM bytes per launch from the committed ncu summary, if one exists for this workload."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return d.get(workload_name, {}).get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_baseline(N: int, U: int, rank: int, steps: int):
+    """The reference solver's step (demos/honey/pfc-relax.c over the project FFT
+    shim, all host threads) timed on a bounded sample of the same workload."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "pfc-relax-bench")
+    if not os.path.exists(exe):
+        return None
+    pd, dx, dy, f = workload(N, rank)
+    with tempfile.TemporaryDirectory() as d:
+        ins = ["in%d.n" % u for u in range(U)]
+        for u in range(U):
+            nfile.write_n_header_only(os.path.join(d, ins[u]), N, N, dx, dy)
+        nfile.write_input(os.path.join(d, "x.in"), ins, ["o%d" % u for u in range(U)], Tprint=10 ** 9,
+                          Twrite=10 ** 9, params=pd, c=1.0, tend=10 ** 6, dx=dx, dy=dy, dt=0.25)
+        np.ascontiguousarray(f, dtype="<f8").tofile(os.path.join(d, "fields.bin"))
+        env = dict(os.environ)
+        threads = os.cpu_count() or 1
+        env["OMP_NUM_THREADS"] = str(threads)
+        r = subprocess.run([exe, "x.in", "fields.bin", "1", str(steps)], cwd=d, capture_output=True, text=True,
+                           env=env, timeout=900)
+        if r.returncode != 0:
+            return {"error": r.stderr[-300:]}
+        res = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": res["steps"] / res["seconds"], "unit": "steps/s", "cores": res["threads"],
+            "kind": "reference",
+            "sample": "%d steps of %dx%d U=%d after 1 warm-up step; reference step() over the project FFT shim "
+                      "(not FFTW), %d OpenMP threads in the FFT, pointwise loops single-threaded"
+                      % (res["steps"], N, N, U, res["threads"])}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU implementation of the step."""
+    if rank != 0:
+        return
+    N, U = args.size, 2
+    steps = max(2, min(args.steps, args.cpu_steps))
+    per = []
+    for _ in range(max(1, args.reps)):
+        cb = cpu_baseline(N, U, rank, steps)
+        if cb is None or "error" in cb:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pfc-relax-bench missing or failed: %s"
+                              % (cb or {}).get("error", "not built")}))
+            return
+        per.append(cb)
+    v = statistics.median(c["value"] for c in per)
+    cb = per[0]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
+            "steps": steps, "warmup": 1, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "hetero2c_%dx%d" % (N, N), "U": U, "grid": [N, N], "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cb["cores"], "kind": "reference",
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--cpu-steps", type=int, default=6, help="reference steps in the CPU sample")
+    ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    lib.set_device(local)
+    torch.cuda.init()
+
+    N, U = args.size, 2
+    pd, dx, dy, f0 = workload(N, rank)
+    params = P.make_params(pd, 1.0, 0.25)
+    Hspec = (N // 2 + 1) * N
+
+    def timed_steps(r: lib.Relaxation, K: int):
+        stream = torch.cuda.ExternalStream(r.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = r.launches
+        e0.record(stream)
+        r.step(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, r.launches - l0
+
+    results = {}
+    precisions = [args.precision] + ([] if args.no_fp64 or args.precision == "fp64" else ["fp64"])
+    for prec in precisions:
+        r = lib.Relaxation(params, N, N, dx, dy, prec)
+        r.upload(f0)
+        r.step(args.warmup)
+        with Clocks(local) as clk:
+            ms, nl = timed_steps(r, args.steps)
+        clocks = clk.summary()
+        # per-kernel durations (events on the library stream), separate run
+        r.set_profiling(True)
+        r.step(min(args.steps, 100))
+        prof = r.profile()
+        r.set_profiling(False)
+        fave, nave = r.evaluate()
+        results[prec] = dict(ms=ms, launches=nl, clocks=clocks, prof=prof, fave=fave, nave=list(nave), r=r)
+
+    main_p = args.precision
+    res = results[main_p]
+    ms = res["ms"]
+    steps_per_s = args.steps * 1000.0 / ms * world
+    eb = 4 if main_p == "fp32" else 8
+    # algorithmic bytes (complex elements of 2*eb bytes): y-pass reads work and
+    # spec, writes spec and work (4 per point); x-pass reads and writes work (2)
+    bytes_y = 4 * 2 * eb * U * Hspec
+    bytes_x = 2 * 2 * eb * U * Hspec
+    prof = res["prof"]
+    kx_ms = prof["xpass"][0] / max(prof["xpass"][1], 1)
+    ky_ms = prof["ypass"][0] / max(prof["ypass"][1], 1)
+    # dominant kernel: the one with the longer time per step
+    dom, dom_ms, dom_bytes = ("ypass", ky_ms, bytes_y) if ky_ms >= kx_ms else ("xpass", kx_ms, bytes_x)
+    peak, peak_kind = hbm_peak()
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    wl_name = "hetero2c_%dx%d_%s" % (N, N, main_p)
+
+    # end to end through the C ABI with host buffers: upload from pinned host
+    # memory, the K steps, the printed energy (device -> host), download
+    r = res["r"]
+    host_in = torch.from_numpy(np.ascontiguousarray(f0)).pin_memory()
+    host_out = torch.empty((U, N, N), dtype=torch.float64).pin_memory()
+    hin = host_in.numpy()
+    hout = host_out.numpy()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r.upload(hin)
+    r.step(args.steps)
+    r.evaluate()
+    r.download(hout)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": args.steps / e2e_s * world, "unit": "steps/s",
+           "h2d_bytes_per_step": int(hin.nbytes / args.steps),
+           "d2h_bytes_per_step": int((hout.nbytes + 8 * (1 + U)) / args.steps),
+           "note": "one relaxation call sequence per run: upload, %d steps, evaluate, download" % args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(N, U, rank, args.cpu_steps)
+
+    line = {
+        "metric": METRIC, "value": steps_per_s, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if main_p == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": wl_name, "U": U, "grid": [N, N], "dt": 0.25, "dynamics": "conserved",
+                   "precision": main_p + " FFT/pointwise, fp64 reductions and k=0 mode",
+                   "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 (268 MB working set)"},
+        "gpu_launches": res["launches"],
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
+                     "traffic": traffic_from_profiles(dom, wl_name),
+                     "step_frac": (bytes_x + bytes_y) / (ms / args.steps * 1e-3) / 1e9 / peak},
+        "kernels_ms": {"xpass": kx_ms, "ypass": ky_ms},
+        "clocks": res["clocks"],
+        "e2e": e2e,
+        "energy": {"fave": res["fave"], "nave": res["nave"]},
+    }
+    if "fp64" in results and main_p != "fp64":
+        r64 = results["fp64"]
+        line["fp64"] = {"steps_per_s": args.steps * 1000.0 / r64["ms"] * world, "ms_per_step": r64["ms"] / args.steps,
+                        "fave": r64["fave"], "rel_dF_vs_fp32": abs(res["fave"] - r64["fave"]) / abs(r64["fave"])}
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line))
+    for v in results.values():
+        v["r"].close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -115,6 +115,19 @@ int pfcg_evaluate(pfcg_handle* h, double* fave, double* nave, double* f);
  * *d is the sampling step (in/out; relax() starts it at 1e-4, :1296). */
 int pfcg_optimize(pfcg_handle* h, int xopt, int yopt, double* d);
 
+/* Makes `device` the CUDA device that later pfcg_create calls on this host
+ * thread use (one process per GPU). No counterpart in the reference, whose
+ * ranks are MPI processes (pfc-relax.c:1395-1401). */
+int pfcg_set_device(int device);
+
+/* Per-kernel timing with CUDA events on the handle's stream (off by default).
+ * pfcg_profile_read returns, for each kernel kind k (0 = x-pass step, 1 = y-pass
+ * step, 2 = everything else), the summed milliseconds and launch counts since
+ * profiling was switched on. No counterpart in the reference (it prints only
+ * wall seconds, pfc-relax.c:881). */
+int pfcg_set_profiling(pfcg_handle* h, int on);
+int pfcg_profile_read(pfcg_handle* h, double* ms, long long* launches, int nkinds);
+
 /* The CUDA stream the handle launches on (a cudaStream_t), for timing. */
 int pfcg_stream(const pfcg_handle* h, void** stream);
 

@@ -1,0 +1,741 @@
+// C ABI of libpfc_b200.so (declared in include/pfc_b200.h): handle life
+// cycle, launch-shape selection and the host side of evaluate / optimize.
+//
+// Reference correspondence (demos/honey/pfc-relax.c):
+//   pfcg_create     allocate_data :162-193, plan_FFTs :196-239, update_AB :901-958
+//   pfcg_upload     read_data's m[u] :729-764 + first resync in step :1179-1185
+//   pfcg_step       step :1134-1248 (x-pass + y-pass kernels per step)
+//   pfcg_evaluate   evaluate :988-1131 (local terms in real space, gradient and
+//                   smoothing terms by Parseval in k space)
+//   pfcg_optimize   optimize :1251-1290
+//   pfcg_download   the m[u] written by write_data :767-815
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pfc_b200.h"
+#include "kernels.cuh"
+
+using namespace pfcg;
+
+namespace {
+
+constexpr int ACC_NL = 0;     // U doubles: sum of the nonlinear term of the current step
+constexpr int ACC_EVAL = 8;   // 1 + U doubles: sum of local energy density, sums of m_u
+constexpr int ACC_TRIAL = 16; // MAX_TRIAL doubles: Parseval sums per box size
+constexpr int ACC_N = 24;
+constexpr int OFFS_N = 32;    // per-field offsets for the f(r) fields
+constexpr int MAX_THREADS = 512;
+constexpr double PI = 3.14159265358979323846264338327;
+
+thread_local std::string g_err;
+
+} // namespace
+
+struct pfcg_handle {
+	int dev = 0;
+	pfcg_prec prec = PFCG_FP64;
+	Model model{};
+	Geom geom{};
+	int U = 0, Nx = 0, Ny = 0, H = 0;
+	int t = 0;
+	cudaStream_t stream = nullptr;
+	size_t celem = 0; // bytes of one complex element
+	void* spec = nullptr;
+	void* work = nullptr;
+	void* work1 = nullptr;
+	void* twx = nullptr;
+	void* twy = nullptr;
+	double* mean = nullptr;
+	double* acc = nullptr;
+	double* offs = nullptr;
+	int* flag = nullptr;
+	int* h_flag = nullptr;
+	double* h_buf = nullptr; // pinned: ACC_N accumulators, MAXU means, OFFS_N offsets
+	FftPlan px{}, py{};
+	LaunchCfg cx{}, cy{}, cx1{}, cy1{};
+	int sbx = 1, sby = 1, sbx1 = 1, sby1 = 1;
+	double* d_real = nullptr;   // U*Ny*Nx doubles
+	double* d_fields = nullptr; // f(r) work fields
+	double* d_part = nullptr;   // partial sums of the field means
+	long long launches = 0;
+	// per-kernel timing (pfcg_set_profiling)
+	bool profiling = false;
+	std::vector<cudaEvent_t> ev;     // event pairs, recorded around launches
+	std::vector<int> ev_kind;
+	double prof_ms[3] = {0, 0, 0};
+	long long prof_n[3] = {0, 0, 0};
+	std::string err;
+};
+
+namespace {
+
+int fail(pfcg_handle* h, int code, const std::string& msg) {
+	if (h) h->err = msg;
+	else g_err = msg;
+	return code;
+}
+
+int cuda_fail(pfcg_handle* h, const char* what, cudaError_t e) {
+	return fail(h, PFCG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(h, call)                                                                                                    \
+	do {                                                                                                           \
+		cudaError_t e_ = (call);                                                                               \
+		if (e_ != cudaSuccess) return cuda_fail(h, #call, e_);                                                 \
+	} while (0)
+
+bool factor_ok(int n) {
+	if (n < 1) return false;
+	for (int f : {2, 3, 5, 7})
+		while (n % f == 0) n /= f;
+	return n == 1;
+}
+
+// n = RM^nmain * rtail * 3^n3 * 5^n5 * 7^n7, rtail in {1,2,4,8} below RM
+bool make_plan(int n, int rmain, FftPlan* p) {
+	if (!factor_ok(n)) return false;
+	int m = n, k2 = 0;
+	p->n = n;
+	p->n3 = p->n5 = p->n7 = 0;
+	while (m % 2 == 0) { m /= 2; k2++; }
+	while (m % 3 == 0) { m /= 3; p->n3++; }
+	while (m % 5 == 0) { m /= 5; p->n5++; }
+	while (m % 7 == 0) { m /= 7; p->n7++; }
+	const int lg = (rmain == 16) ? 4 : 3;
+	p->nmain = k2 / lg;
+	p->rtail = 1 << (k2 % lg);
+	return true;
+}
+
+// threads one fft_batch over P sequences needs (0 if more than MAX_THREADS)
+int threads_for(const FftPlan& p, int P, int maxe) {
+	auto need = [&](int R) {
+		const long long bfly = (long long)P * p.n / R;
+		const int nb = maxe / R;
+		return (int)((bfly + nb - 1) / nb);
+	};
+	int nt = 32;
+	if (p.nmain > 0) nt = std::max(nt, need(maxe));
+	if (p.rtail > 1) nt = std::max(nt, need(p.rtail));
+	if (p.n3) nt = std::max(nt, need(3));
+	if (p.n5) nt = std::max(nt, need(5));
+	if (p.n7) nt = std::max(nt, need(7));
+	nt = (nt + 31) / 32 * 32;
+	return nt <= MAX_THREADS ? nt : 0;
+}
+
+// largest sub-batch (<= S) whose FFT fits in MAX_THREADS threads; 0 if none
+int sub_batch(const FftPlan& p, int S, int maxe, int* nt) {
+	for (int sb = S; sb >= 1; sb--) {
+		const int t = threads_for(p, sb, maxe);
+		if (t) { *nt = t; return sb; }
+	}
+	return 0;
+}
+
+template <typename T> int padded_host(int n) { return padded_len<T>(n); }
+
+int padded(int n, bool fp64) { return fp64 ? padded_host<double>(n) : padded_host<float>(n); }
+
+// Chooses the row tile R (x-pass) and column group CC (y-pass): the largest
+// sizes that fit shared memory and still give at least two CTAs per SM.
+int choose_layout(pfcg_handle* h, int nsm) {
+	const bool fp64 = h->prec == PFCG_FP64;
+	const int maxe = max_elems_per_thread(fp64);
+	const size_t budget = fp64 ? 200 * 1024 : 150 * 1024;
+	const int want = 2 * nsm;
+	const int U = h->U;
+	int R = 0;
+	for (int r : {8, 4, 2, 1}) {
+		if (h->Ny % r) continue;
+		const int CH = U * r;
+		if (CH > MAX_CH) continue;
+		const int P = (CH + 1) / 2;
+		if ((size_t)P * padded(h->Nx, fp64) * h->celem > budget) continue;
+		int nt;
+		if (!sub_batch(h->px, P, maxe, &nt)) continue;
+		R = r;
+		if (h->Ny / r >= want) break;
+	}
+	if (!R) return fail(h, PFCG_ESIZE, "no x-pass tile fits shared memory for this Nx");
+	int CC = 0;
+	for (int c : {4, 2, 1}) {
+		const int S = U * c;
+		if ((size_t)S * padded(h->Ny, fp64) * h->celem > budget) continue;
+		int nt;
+		if (!sub_batch(h->py, S, maxe, &nt)) continue;
+		CC = c;
+		if ((h->H + c - 1) / c >= want) break;
+	}
+	if (!CC) return fail(h, PFCG_ESIZE, "no y-pass column group fits shared memory for this Ny");
+	h->geom.R = R;
+	h->geom.CC = CC;
+
+	int nt;
+	const int P = (U * R + 1) / 2;
+	h->sbx = sub_batch(h->px, P, maxe, &nt);
+	h->cx = {h->Ny / R, nt, (int)(P * padded(h->Nx, fp64) * h->celem)};
+	const int P1 = (R + 1) / 2;
+	h->sbx1 = sub_batch(h->px, P1, maxe, &nt);
+	h->cx1 = {h->Ny / R, nt, (int)(P1 * padded(h->Nx, fp64) * h->celem)};
+	const int S = U * CC;
+	h->sby = sub_batch(h->py, S, maxe, &nt);
+	h->cy = {(h->H + CC - 1) / CC, nt, (int)(S * padded(h->Ny, fp64) * h->celem)};
+	h->sby1 = sub_batch(h->py, CC, maxe, &nt);
+	h->cy1 = {(h->H + CC - 1) / CC, nt, (int)(CC * padded(h->Ny, fp64) * h->celem)};
+	return 0;
+}
+
+template <typename T> int upload_twiddles(pfcg_handle* h, int n, void** dst) {
+	std::vector<cplx<T>> tw(n);
+	for (int k = 0; k < n; k++) {
+		const double a = -2.0 * PI * (double)k / (double)n;
+		tw[k].x = (T)std::cos(a);
+		tw[k].y = (T)std::sin(a);
+	}
+	CK(h, cudaMalloc(dst, sizeof(cplx<T>) * n));
+	CK(h, cudaMemcpy(*dst, tw.data(), sizeof(cplx<T>) * n, cudaMemcpyHostToDevice));
+	return 0;
+}
+
+Model to_model(const pfcg_params* p) {
+	Model m{};
+	m.U = p->U;
+	for (int u = 0; u < MAXU; u++) {
+		m.W[u] = u < p->U ? p->W[u] : 0;
+		m.lambda[u] = p->lambda[u];
+		m.delta[u] = p->delta[u];
+		for (int v = 0; v < MAXU; v++) {
+			m.alpha[u][v] = p->alpha[u][v];
+			m.beta[u][v] = p->beta[u][v];
+			m.gamma[u][v] = p->gamma[u][v];
+			m.epsilon[u][v] = p->epsilon[u][v];
+			m.mu2[u][v] = p->mu2[u][v];
+		}
+		for (int w = 0; w < MAXW; w++) {
+			m.nu2[u][w] = p->nu2[u][w];
+			m.omega[u][w] = p->omega[u][w];
+			m.phi[u][w] = p->phi[u][w];
+		}
+	}
+	m.c = (p->c != 0.0) ? 1.0 : 0.0; // pfc-relax.c:930
+	m.sigma = p->sigma;
+	m.dt = p->dt;
+	return m;
+}
+
+double P_host(const Model& m, int u, double k2) {
+	double P = 1.0;
+	for (int w = 0; w < m.W[u]; w++) {
+		const double q = m.nu2[u][w] - k2;
+		P *= m.omega[u][w] * q * q + m.phi[u][w];
+	}
+	return P;
+}
+
+// k = 0 term of the Parseval sum (the mean is held outside the spectrum)
+double k0_energy(const Model& m, const double* mean) {
+	double e = 0.0;
+	for (int u = 0; u < m.U; u++) {
+		e += 0.5 * m.beta[u][u] * P_host(m, u, 0.0) * mean[u] * mean[u];
+		for (int v = u + 1; v < m.U; v++)
+			e += (m.beta[u][v] * m.mu2[u][v] * m.mu2[u][v] + m.epsilon[u][v]) * mean[u] * mean[v];
+	}
+	return e;
+}
+
+template <typename T> XArgs<T> xargs(pfcg_handle* h) {
+	XArgs<T> a{};
+	a.work = (cplx<T>*)h->work;
+	a.wstride = (long long)h->H * h->Ny;
+	a.off = h->mean;
+	a.real = h->d_real;
+	a.acc = h->acc;
+	a.flag = h->flag;
+	a.tw = (const cplx<T>*)h->twx;
+	a.plan = h->px;
+	a.sb = h->sbx;
+	a.m = h->model;
+	a.g = h->geom;
+	return a;
+}
+
+template <typename T> YArgs<T> yargs(pfcg_handle* h) {
+	YArgs<T> a{};
+	a.work = (cplx<T>*)h->work;
+	a.wstride = (long long)h->H * h->Ny;
+	a.spec = (cplx<T>*)h->spec;
+	a.sstride = (long long)h->H * h->Ny;
+	a.mean = h->mean;
+	a.acc = h->acc + ACC_NL;
+	a.tw = (const cplx<T>*)h->twy;
+	a.plan = h->py;
+	a.sb = h->sby;
+	a.m = h->model;
+	a.g = h->geom;
+	return a;
+}
+
+constexpr int MEAN_BLOCKS = 296;
+
+// Event pair around a launch when profiling; kind 0 = x-pass step, 1 = y-pass step, 2 = other.
+struct ProfScope {
+	pfcg_handle* h;
+	int kind;
+	cudaEvent_t b = nullptr, e = nullptr;
+	ProfScope(pfcg_handle* h_, int k) : h(h_), kind(k) {
+		if (!h->profiling) return;
+		cudaEventCreate(&b);
+		cudaEventCreate(&e);
+		cudaEventRecord(b, h->stream);
+	}
+	~ProfScope() {
+		if (!b) return;
+		cudaEventRecord(e, h->stream);
+		h->ev.push_back(b);
+		h->ev.push_back(e);
+		h->ev_kind.push_back(kind);
+	}
+};
+
+void profile_collect(pfcg_handle* h) {
+	if (h->ev.empty()) return;
+	cudaStreamSynchronize(h->stream);
+	for (size_t i = 0; i < h->ev_kind.size(); i++) {
+		float ms = 0.f;
+		cudaEventElapsedTime(&ms, h->ev[2 * i], h->ev[2 * i + 1]);
+		h->prof_ms[h->ev_kind[i]] += ms;
+		h->prof_n[h->ev_kind[i]]++;
+		cudaEventDestroy(h->ev[2 * i]);
+		cudaEventDestroy(h->ev[2 * i + 1]);
+	}
+	h->ev.clear();
+	h->ev_kind.clear();
+}
+
+int ensure_real(pfcg_handle* h) {
+	if (!h->d_real) CK(h, cudaMalloc(&h->d_real, sizeof(double) * (size_t)h->U * h->Nx * h->Ny));
+	return 0;
+}
+
+template <typename T> int run_xpass(pfcg_handle* h, int mode, const XArgs<T>& a, const LaunchCfg& c) {
+	h->launches++;
+	ProfScope ps(h, mode == XP_STEP ? 0 : 2);
+	CK(h, launch_xpass<T>(mode, a, c, h->stream));
+	return 0;
+}
+template <typename T> int run_ypass(pfcg_handle* h, int mode, const YArgs<T>& a, const LaunchCfg& c) {
+	h->launches++;
+	ProfScope ps(h, mode == YP_STEP ? 1 : 2);
+	CK(h, launch_ypass<T>(mode, a, c, h->stream));
+	return 0;
+}
+
+template <typename T> int do_upload(pfcg_handle* h, const double* fields) {
+	int rc = ensure_real(h);
+	if (rc) return rc;
+	const size_t npts = (size_t)h->Nx * h->Ny;
+	CK(h, cudaMemcpyAsync(h->d_real, fields, sizeof(double) * h->U * npts, cudaMemcpyHostToDevice, h->stream));
+	// the mean (k = 0 mode) in FP64, by a fixed-order reduction on the device
+	h->launches += 2;
+	{
+		ProfScope ps(h, 2);
+		CK(h, launch_field_means(h->d_real, h->U, (long long)npts, h->d_part, MEAN_BLOCKS, h->mean, h->stream));
+	}
+	XArgs<T> xa = xargs<T>(h);
+	rc = run_xpass<T>(h, XP_R2C, xa, h->cx);
+	if (rc) return rc;
+	YArgs<T> ya = yargs<T>(h);
+	rc = run_ypass<T>(h, YP_INIT, ya, h->cy);
+	if (rc) return rc;
+	CK(h, cudaStreamSynchronize(h->stream));
+	h->t = 0;
+	return 0;
+}
+
+template <typename T> int do_download(pfcg_handle* h, double* fields) {
+	int rc = ensure_real(h);
+	if (rc) return rc;
+	XArgs<T> xa = xargs<T>(h);
+	rc = run_xpass<T>(h, XP_C2R, xa, h->cx);
+	if (rc) return rc;
+	CK(h, cudaMemcpyAsync(fields, h->d_real, sizeof(double) * h->U * (size_t)h->Nx * h->Ny, cudaMemcpyDeviceToHost,
+	                      h->stream));
+	CK(h, cudaStreamSynchronize(h->stream));
+	return 0;
+}
+
+template <typename T> int do_steps(pfcg_handle* h, int nsteps) {
+	XArgs<T> xa = xargs<T>(h);
+	xa.acc = h->acc + ACC_NL;
+	YArgs<T> ya = yargs<T>(h);
+	// The reference resynchronises the spectral state every 100 steps and after
+	// evaluate (pfc-relax.c:1179-1185, 1125-1130); the y-pass does the same
+	// projection every step, so no separate pass is needed.
+	for (int s = 0; s < nsteps; s++) {
+		int rc = run_xpass<T>(h, XP_STEP, xa, h->cx);
+		if (rc) return rc;
+		rc = run_ypass<T>(h, YP_STEP, ya, h->cy);
+		if (rc) return rc;
+		h->t++;
+	}
+	CK(h, cudaMemcpyAsync(h->h_flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+	CK(h, cudaStreamSynchronize(h->stream));
+	if (*h->h_flag) return fail(h, PFCG_NAN, "Not a number value detected.");
+	return 0;
+}
+
+// local part (real space) and Parseval part for ntrial box sizes; returns
+// host pointers to the accumulators (valid until the next call)
+template <typename T> int eval_sums(pfcg_handle* h, int ntrial, const double* dxs, const double* dys, bool local) {
+	CK(h, cudaMemsetAsync(h->acc + ACC_EVAL, 0, sizeof(double) * 16, h->stream));
+	if (local) {
+		XArgs<T> xa = xargs<T>(h);
+		xa.acc = h->acc + ACC_EVAL;
+		int rc = run_xpass<T>(h, XP_EVAL, xa, h->cx);
+		if (rc) return rc;
+	}
+	h->launches++;
+	ProfScope ps(h, 2);
+	CK(h, launch_kspace_energy<T>((const cplx<T>*)h->spec, (long long)h->H * h->Ny, h->model, h->geom, ntrial, dxs, dys,
+	                              h->acc + ACC_TRIAL, h->stream));
+	CK(h, cudaMemcpyAsync(h->h_buf, h->acc, sizeof(double) * ACC_N, cudaMemcpyDeviceToHost, h->stream));
+	CK(h, cudaMemcpyAsync(h->h_buf + ACC_N, h->mean, sizeof(double) * h->U, cudaMemcpyDeviceToHost, h->stream));
+	CK(h, cudaStreamSynchronize(h->stream));
+	return 0;
+}
+
+template <typename T> int energy_field(pfcg_handle* h, double* f_host) {
+	const long long npts = (long long)h->Nx * h->Ny;
+	const int U = h->U;
+	const int npair = U * (U - 1) / 2;
+	const int nf = 3 * U + npair + 1;
+	if (!h->d_fields) CK(h, cudaMalloc(&h->d_fields, sizeof(double) * npts * nf));
+	if (!h->work1) CK(h, cudaMalloc(&h->work1, h->celem * (size_t)h->H * h->Ny));
+	double* mf = h->d_fields;
+	double* pn = mf + U * npts;
+	double* eta = pn + U * npts;
+	double* q = eta + U * npts;
+	double* f = q + npair * npts;
+	const double* hm = h->h_buf + ACC_N; // means, fetched by eval_sums
+	double* ho = h->h_buf + ACC_N + MAXU;
+	// offsets = weight at k = 0 times the mean
+	int k = 0;
+	for (int u = 0; u < U; u++) ho[k++] = P_host(h->model, u, 0.0) * hm[u];
+	for (int u = 0; u < U; u++) ho[k++] = hm[u];
+	for (int u = 0; u < U; u++)
+		for (int v = u + 1; v < U; v++) ho[k++] = h->model.mu2[u][v] * h->model.mu2[u][v] * hm[v];
+	CK(h, cudaMemcpyAsync(h->offs, ho, sizeof(double) * k, cudaMemcpyHostToDevice, h->stream));
+
+	XArgs<T> xa = xargs<T>(h);
+	xa.real = mf;
+	int rc = run_xpass<T>(h, XP_C2R, xa, h->cx);
+	if (rc) return rc;
+
+	auto weighted = [&](int kind, int src, int u, int v, double* out, int oi) -> int {
+		YArgs<T> ya = yargs<T>(h);
+		ya.work = (cplx<T>*)h->work1;
+		ya.sb = h->sby1;
+		ya.wkind = kind;
+		ya.wsrc = src;
+		ya.wp = WParams{};
+		ya.wp.W = h->model.W[u];
+		for (int w = 0; w < MAXW; w++) {
+			ya.wp.nu2[w] = h->model.nu2[u][w];
+			ya.wp.omega[w] = h->model.omega[u][w];
+			ya.wp.phi[w] = h->model.phi[u][w];
+		}
+		ya.wp.mu2 = (v >= 0) ? h->model.mu2[u][v] : 0.0;
+		int r = run_ypass<T>(h, YP_WEIGHT, ya, h->cy1);
+		if (r) return r;
+		XArgs<T> x1 = xargs<T>(h);
+		x1.work = (cplx<T>*)h->work1;
+		x1.m.U = 1;
+		x1.sb = h->sbx1;
+		x1.off = h->offs + oi;
+		x1.real = out;
+		return run_xpass<T>(h, XP_C2R, x1, h->cx1);
+	};
+	k = 0;
+	for (int u = 0; u < U; u++, k++)
+		if ((rc = weighted(W_P, u, u, -1, pn + u * npts, k))) return rc;
+	for (int u = 0; u < U; u++, k++)
+		if ((rc = weighted(W_G, u, u, -1, eta + u * npts, k))) return rc;
+	int pair = 0;
+	for (int u = 0; u < U; u++)
+		for (int v = u + 1; v < U; v++, pair++, k++)
+			if ((rc = weighted(W_Q, v, u, v, q + pair * npts, k))) return rc;
+	h->launches++;
+	CK(h, launch_energy_density(mf, pn, eta, q, npair, h->model, npts, f, h->stream));
+	CK(h, cudaMemcpyAsync(f_host, f, sizeof(double) * npts, cudaMemcpyDeviceToHost, h->stream));
+	CK(h, cudaStreamSynchronize(h->stream));
+	return 0;
+}
+
+template <typename T> int do_evaluate(pfcg_handle* h, double* fave, double* nave, double* f) {
+	const double dx = h->geom.dx, dy = h->geom.dy;
+	int rc = eval_sums<T>(h, 1, &dx, &dy, true);
+	if (rc) return rc;
+	const double N = (double)h->Nx * h->Ny;
+	const double* acc = h->h_buf;
+	const double* hm = h->h_buf + ACC_N;
+	const double Q = acc[ACC_TRIAL] + k0_energy(h->model, hm);
+	if (fave) *fave = acc[ACC_EVAL] / N + Q;
+	// <n_u> is the k = 0 mode, held in FP64 (the reference sums n over the grid,
+	// pfc-relax.c:1114, which is the same number up to rounding)
+	if (nave)
+		for (int u = 0; u < h->U; u++) nave[u] = hm[u];
+	if (f) {
+		rc = energy_field<T>(h, f);
+		if (rc) return rc;
+	}
+	return 0;
+}
+
+template <typename T> int do_optimize(pfcg_handle* h, int xopt, int yopt, double* d) {
+	const double dx0 = h->geom.dx, dy0 = h->geom.dy;
+	const double dxs[5] = {dx0, dx0 - *d, dx0 + *d, dx0, dx0};
+	const double dys[5] = {dy0, dy0, dy0, dy0 - *d, dy0 + *d};
+	int idx[5], n = 0;
+	double tx[5], ty[5];
+	for (int i = 0; i < 5; i++) {
+		if (xopt == 0 && (i == 1 || i == 2)) continue;
+		if (yopt == 0 && (i == 3 || i == 4)) continue;
+		idx[n] = i;
+		tx[n] = dxs[i];
+		ty[n] = dys[i];
+		n++;
+	}
+	int rc = eval_sums<T>(h, n, tx, ty, true);
+	if (rc) return rc;
+	const double N = (double)h->Nx * h->Ny;
+	const double* acc = h->h_buf;
+	const double k0 = k0_energy(h->model, h->h_buf + ACC_N);
+	double fs[5] = {0, 0, 0, 0, 0};
+	for (int i = 0; i < n; i++) fs[idx[i]] = acc[ACC_EVAL] / N + acc[ACC_TRIAL + i] + k0;
+	// the reference leaves s->dx, s->dy at the last sampled size (:1260-1267)
+	double dx = tx[n - 1], dy = ty[n - 1];
+	if (xopt != 0) dx = (*d * (fs[1] - fs[2]) + 2.0 * dxs[0] * (-2.0 * fs[0] + fs[1] + fs[2])) / (2.0 * (fs[1] - 2.0 * fs[0] + fs[2]));
+	if (yopt != 0) dy = (*d * (fs[3] - fs[4]) + 2.0 * dys[0] * (-2.0 * fs[0] + fs[3] + fs[4])) / (2.0 * (fs[3] - 2.0 * fs[0] + fs[4]));
+	const double l0 = 4.0 * PI / std::sqrt(3.0);
+	const double dw = h->Nx * (dx - dxs[0]);
+	const double dh = h->Ny * (dy - dys[0]);
+	const double dr = std::sqrt(dw * dw + dh * dh);
+	double x = 0.25 * l0;
+	if (dr > x) {
+		x /= dr;
+		dx = x * dx + (1.0 - x) * dxs[0];
+		dy = x * dy + (1.0 - x) * dys[0];
+	}
+	h->geom.dx = dx;
+	h->geom.dy = dy;
+	const double ddx = dx - dxs[0], ddy = dy - dys[0];
+	const double ddr = std::sqrt(ddx * ddx + ddy * ddy);
+	if (ddr < *d) *d *= 0.5;
+	else *d *= 2.0;
+	if (*d < 1.0e-6) *d *= 2.0;
+	return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int pfcg_size_supported(int Nx, int Ny) {
+	if (Nx < 8 || Ny < 8 || Nx > 8192 || Ny > 8192) return 0;
+	if (Nx % 2 || Ny % 2) return 0;
+	return factor_ok(Nx) && factor_ok(Ny);
+}
+
+int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg_prec prec, pfcg_handle** out) {
+	if (!out) return fail(nullptr, PFCG_EARG, "out is NULL");
+	*out = nullptr;
+	if (!p) return fail(nullptr, PFCG_EARG, "params is NULL");
+	if (p->U < 1 || p->U > PFCG_MAX_U) return fail(nullptr, PFCG_EARG, "U out of range 1..4");
+	for (int u = 0; u < p->U; u++)
+		if (p->W[u] < 0 || p->W[u] > PFCG_MAX_W) return fail(nullptr, PFCG_EARG, "W[u] out of range 0..4");
+	if (prec != PFCG_FP32 && prec != PFCG_FP64) return fail(nullptr, PFCG_EARG, "unknown precision");
+	if (!pfcg_size_supported(Nx, Ny))
+		return fail(nullptr, PFCG_ESIZE, "grid size not supported (need even 8..8192 with factors 2,3,5,7)");
+
+	int dev = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e != cudaSuccess) return fail(nullptr, PFCG_ENODEV, std::string("no CUDA device: ") + cudaGetErrorString(e));
+	cudaDeviceProp prop;
+	e = cudaGetDeviceProperties(&prop, dev);
+	if (e != cudaSuccess) return fail(nullptr, PFCG_ENODEV, cudaGetErrorString(e));
+	if (prop.major != 10) return fail(nullptr, PFCG_ENODEV, "libpfc_b200 is built for sm_100a (B200) only");
+
+	pfcg_handle* h = new pfcg_handle();
+	h->dev = dev;
+	h->prec = prec;
+	h->model = to_model(p);
+	h->U = p->U;
+	h->Nx = Nx;
+	h->Ny = Ny;
+	h->H = Nx / 2 + 1;
+	h->geom.Nx = Nx;
+	h->geom.Ny = Ny;
+	h->geom.H = h->H;
+	h->geom.dx = dx;
+	h->geom.dy = dy;
+	const bool fp64 = prec == PFCG_FP64;
+	h->celem = fp64 ? sizeof(double2) : sizeof(float2);
+	const int rmain = max_radix(fp64);
+	int rc = 0;
+	if (!make_plan(Nx, rmain, &h->px) || !make_plan(Ny, rmain, &h->py)) rc = fail(h, PFCG_ESIZE, "bad factorisation");
+	if (!rc) rc = choose_layout(h, prop.multiProcessorCount);
+	auto bail = [&](int code) {
+		g_err = h->err;
+		pfcg_destroy(h);
+		return code;
+	};
+	if (rc) return bail(rc);
+	const size_t nspec = (size_t)h->H * Ny;
+#define CKC(call)                                                                                                      \
+	do {                                                                                                           \
+		cudaError_t e_ = (call);                                                                               \
+		if (e_ != cudaSuccess) return bail(cuda_fail(h, #call, e_));                                           \
+	} while (0)
+	CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+	CKC(cudaMalloc(&h->spec, h->celem * nspec * h->U));
+	CKC(cudaMalloc(&h->work, h->celem * nspec * h->U));
+	CKC(cudaMalloc(&h->mean, sizeof(double) * MAXU));
+	CKC(cudaMalloc(&h->acc, sizeof(double) * ACC_N));
+	CKC(cudaMalloc(&h->offs, sizeof(double) * OFFS_N));
+	CKC(cudaMalloc(&h->flag, sizeof(int)));
+	CKC(cudaMalloc(&h->d_part, sizeof(double) * MAXU * MEAN_BLOCKS));
+	CKC(cudaMallocHost(&h->h_flag, sizeof(int)));
+	CKC(cudaMallocHost(&h->h_buf, sizeof(double) * (ACC_N + MAXU + OFFS_N)));
+	CKC(cudaMemset(h->spec, 0, h->celem * nspec * h->U));
+	CKC(cudaMemset(h->work, 0, h->celem * nspec * h->U));
+	CKC(cudaMemset(h->mean, 0, sizeof(double) * MAXU));
+	CKC(cudaMemset(h->acc, 0, sizeof(double) * ACC_N));
+	CKC(cudaMemset(h->flag, 0, sizeof(int)));
+#undef CKC
+	rc = fp64 ? upload_twiddles<double>(h, Nx, &h->twx) : upload_twiddles<float>(h, Nx, &h->twx);
+	if (!rc) rc = fp64 ? upload_twiddles<double>(h, Ny, &h->twy) : upload_twiddles<float>(h, Ny, &h->twy);
+	if (rc) return bail(rc);
+	*out = h;
+	return 0;
+}
+
+void pfcg_destroy(pfcg_handle* h) {
+	if (!h) return;
+	if (h->stream) cudaStreamSynchronize(h->stream);
+	cudaFree(h->spec);
+	cudaFree(h->work);
+	cudaFree(h->work1);
+	cudaFree(h->twx);
+	cudaFree(h->twy);
+	cudaFree(h->mean);
+	cudaFree(h->acc);
+	cudaFree(h->offs);
+	cudaFree(h->flag);
+	cudaFree(h->d_real);
+	cudaFree(h->d_fields);
+	cudaFree(h->d_part);
+	for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+	if (h->h_flag) cudaFreeHost(h->h_flag);
+	if (h->h_buf) cudaFreeHost(h->h_buf);
+	if (h->stream) cudaStreamDestroy(h->stream);
+	delete h;
+}
+
+int pfcg_upload(pfcg_handle* h, const double* fields) {
+	if (!h || !fields) return fail(h, PFCG_EARG, "NULL argument");
+	return h->prec == PFCG_FP64 ? do_upload<double>(h, fields) : do_upload<float>(h, fields);
+}
+
+int pfcg_download(pfcg_handle* h, double* fields) {
+	if (!h || !fields) return fail(h, PFCG_EARG, "NULL argument");
+	return h->prec == PFCG_FP64 ? do_download<double>(h, fields) : do_download<float>(h, fields);
+}
+
+int pfcg_set_box(pfcg_handle* h, double dx, double dy) {
+	if (!h) return PFCG_EARG;
+	h->geom.dx = dx;
+	h->geom.dy = dy;
+	return 0;
+}
+
+int pfcg_get_box(const pfcg_handle* h, double* dx, double* dy) {
+	if (!h || !dx || !dy) return PFCG_EARG;
+	*dx = h->geom.dx;
+	*dy = h->geom.dy;
+	return 0;
+}
+
+int pfcg_set_time(pfcg_handle* h, int t) {
+	if (!h) return PFCG_EARG;
+	h->t = t;
+	return 0;
+}
+
+int pfcg_get_time(const pfcg_handle* h, int* t) {
+	if (!h || !t) return PFCG_EARG;
+	*t = h->t;
+	return 0;
+}
+
+int pfcg_step(pfcg_handle* h, int nsteps) {
+	if (!h || nsteps < 0) return fail(h, PFCG_EARG, "bad argument");
+	if (nsteps == 0) return 0;
+	return h->prec == PFCG_FP64 ? do_steps<double>(h, nsteps) : do_steps<float>(h, nsteps);
+}
+
+int pfcg_evaluate(pfcg_handle* h, double* fave, double* nave, double* f) {
+	if (!h) return PFCG_EARG;
+	return h->prec == PFCG_FP64 ? do_evaluate<double>(h, fave, nave, f) : do_evaluate<float>(h, fave, nave, f);
+}
+
+int pfcg_optimize(pfcg_handle* h, int xopt, int yopt, double* d) {
+	if (!h || !d) return fail(h, PFCG_EARG, "NULL argument");
+	return h->prec == PFCG_FP64 ? do_optimize<double>(h, xopt, yopt, d) : do_optimize<float>(h, xopt, yopt, d);
+}
+
+int pfcg_set_device(int device) {
+	cudaError_t e = cudaSetDevice(device);
+	if (e != cudaSuccess) return fail(nullptr, PFCG_ENODEV, cudaGetErrorString(e));
+	return 0;
+}
+
+int pfcg_set_profiling(pfcg_handle* h, int on) {
+	if (!h) return PFCG_EARG;
+	profile_collect(h);
+	h->profiling = on != 0;
+	for (int k = 0; k < 3; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
+	return 0;
+}
+
+int pfcg_profile_read(pfcg_handle* h, double* ms, long long* launches, int nkinds) {
+	if (!h || nkinds < 0) return PFCG_EARG;
+	profile_collect(h);
+	for (int k = 0; k < nkinds && k < 3; k++) {
+		if (ms) ms[k] = h->prof_ms[k];
+		if (launches) launches[k] = h->prof_n[k];
+	}
+	return 0;
+}
+
+int pfcg_stream(const pfcg_handle* h, void** stream) {
+	if (!h || !stream) return PFCG_EARG;
+	*stream = (void*)h->stream;
+	return 0;
+}
+
+int pfcg_launch_count(const pfcg_handle* h, long long* count) {
+	if (!h || !count) return PFCG_EARG;
+	*count = h->launches;
+	return 0;
+}
+
+const char* pfcg_last_error(const pfcg_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+} // extern "C"

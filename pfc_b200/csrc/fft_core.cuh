@@ -1,0 +1,307 @@
+// Shared-memory mixed-radix FFT building blocks for sm_100a.
+//
+// One CTA transforms a batch of P complex sequences of length N that sit in
+// shared memory. Each pass is one radix-R Stockham autosort stage (Govindaraju
+// et al., "High performance discrete Fourier transforms on graphics
+// processors", SC 2008): butterfly j of a sequence reads x[j + r*N/R]
+// (r = 0..R-1, consecutive threads read consecutive words), multiplies by the
+// twiddle W^(r * (j mod Ns) * N/(Ns*R)), does a length-R DFT in registers and
+// writes y[(j/Ns)*Ns*R + (j mod Ns) + r*Ns]. The output comes out in natural
+// order, so no bit reversal is needed.
+//
+// The pass is done in place: every thread first loads all the butterflies it
+// owns into registers, the CTA synchronises, then every thread writes. A
+// thread owns at most MAXE/R butterflies of a pass (MAXE elements).
+//
+// Shared memory is padded by one element every 128 bytes (pad()) so the
+// strided writes of the first passes do not hit one bank.
+//
+// Twiddles come from a per-length table tw[k] = exp(-2 pi i k / N) that the host
+// computes in double precision and stores in the transform precision; the
+// backward transform uses the conjugate.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pfcg {
+
+template <typename T> struct cplx_t;
+template <> struct cplx_t<float> { using type = float2; };
+template <> struct cplx_t<double> { using type = double2; };
+template <typename T> using cplx = typename cplx_t<T>::type;
+
+template <typename T> __host__ __device__ __forceinline__ cplx<T> mk(T x, T y) { cplx<T> r; r.x = x; r.y = y; return r; }
+template <typename V> __host__ __device__ __forceinline__ V cadd(V a, V b) { V r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename V> __host__ __device__ __forceinline__ V csub(V a, V b) { V r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
+	V r;
+	r.x = a.x * b.x - a.y * b.y;
+	r.y = a.x * b.y + a.y * b.x;
+	return r;
+}
+template <typename V> __host__ __device__ __forceinline__ V cconj(V a) { a.y = -a.y; return a; }
+template <typename V, typename T> __host__ __device__ __forceinline__ V cscale(V a, T s) { a.x *= s; a.y *= s; return a; }
+// a * (sign * i)
+template <int SIGN, typename V> __host__ __device__ __forceinline__ V cmul_si(V a) {
+	V r;
+	if (SIGN < 0) { r.x = a.y; r.y = -a.x; }
+	else { r.x = -a.y; r.y = a.x; }
+	return r;
+}
+
+// Padded shared-memory index: one spare element after every 128 bytes.
+template <typename T> struct Pad;
+template <> struct Pad<float> { static constexpr int SHIFT = 4; };
+template <> struct Pad<double> { static constexpr int SHIFT = 3; };
+template <typename T> __device__ __host__ __forceinline__ int pad(int i) { return i + (i >> Pad<T>::SHIFT); }
+template <typename T> __host__ __device__ inline int padded_len(int n) { return n + (n >> Pad<T>::SHIFT) + 1; }
+
+// ---------------------------------------------------------------- DFTs ---
+// In-register DFT of length R: v'[k] = sum_r v[r] exp(SIGN 2 pi i r k / R).
+
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft2(cplx<T>* v) {
+	cplx<T> a = v[0], b = v[1];
+	v[0] = cadd(a, b);
+	v[1] = csub(a, b);
+}
+
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft4(cplx<T>* v) {
+	cplx<T> a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+	cplx<T> b0 = cadd(v[1], v[3]), b1 = cmul_si<SIGN>(csub(v[1], v[3]));
+	v[0] = cadd(a0, b0);
+	v[1] = cadd(a1, b1);
+	v[2] = csub(a0, b0);
+	v[3] = csub(a1, b1);
+}
+
+// length 8 as 2 x 4: inner DFT4 on even/odd halves, twiddle by exp(SIGN 2 pi i k/8)
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft8(cplx<T>* v) {
+	const T h = (T)0.70710678118654752440084436210485; // 1/sqrt(2)
+	cplx<T> e[4] = {v[0], v[2], v[4], v[6]};
+	cplx<T> o[4] = {v[1], v[3], v[5], v[7]};
+	dft4<SIGN, T>(e);
+	dft4<SIGN, T>(o);
+	// o[k] *= exp(SIGN 2 pi i k / 8)
+	o[1] = mk<T>(h * (o[1].x - SIGN * o[1].y), h * (o[1].y + SIGN * o[1].x));
+	o[2] = cmul_si<SIGN>(o[2]);
+	o[3] = mk<T>(h * (-o[3].x - SIGN * o[3].y), h * (-o[3].y + SIGN * o[3].x));
+#pragma unroll
+	for (int k = 0; k < 4; k++) {
+		v[k] = cadd(e[k], o[k]);
+		v[k + 4] = csub(e[k], o[k]);
+	}
+}
+
+// length 16 as 4 x 4 (four DFT4 on stride-4 subsequences, twiddles, four DFT4)
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft16(cplx<T>* v) {
+	const T c1 = (T)0.92387953251128675612818318939679;  // cos(pi/8)
+	const T s1 = (T)0.38268343236508977172845998403040;  // sin(pi/8)
+	const T h = (T)0.70710678118654752440084436210485;   // cos(pi/4)
+	cplx<T> a[4][4];
+#pragma unroll
+	for (int q = 0; q < 4; q++) {
+#pragma unroll
+		for (int r = 0; r < 4; r++) a[q][r] = v[4 * r + q];
+		dft4<SIGN, T>(a[q]);
+	}
+	// a[q][k] *= exp(SIGN 2 pi i q k / 16), q, k in 0..3
+	// q=1: k=1 (c1,s1), k=2 (h,h), k=3 (s1,c1)
+	// q=2: k=1 (h,h), k=2 i, k=3 (-h,h)
+	// q=3: k=1 (s1,c1), k=2 (-h,h), k=3 (-c1,-s1)
+	const T cs[4][4][2] = {
+		{{1, 0}, {1, 0}, {1, 0}, {1, 0}},
+		{{1, 0}, {c1, s1}, {h, h}, {s1, c1}},
+		{{1, 0}, {h, h}, {0, 1}, {-h, h}},
+		{{1, 0}, {s1, c1}, {-h, h}, {-c1, -s1}},
+	};
+#pragma unroll
+	for (int q = 1; q < 4; q++)
+#pragma unroll
+		for (int k = 1; k < 4; k++) {
+			cplx<T> w = mk<T>(cs[q][k][0], SIGN * cs[q][k][1]);
+			a[q][k] = cmul(a[q][k], w);
+		}
+#pragma unroll
+	for (int k = 0; k < 4; k++) {
+		cplx<T> b[4] = {a[0][k], a[1][k], a[2][k], a[3][k]};
+		dft4<SIGN, T>(b);
+#pragma unroll
+		for (int s = 0; s < 4; s++) v[k + 4 * s] = b[s];
+	}
+}
+
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft3(cplx<T>* v) {
+	const T c = (T)-0.5;
+	const T s = (T)SIGN * (T)0.86602540378443864676372317075294; // SIGN sin(2 pi/3)
+	cplx<T> t1 = cadd(v[1], v[2]);
+	cplx<T> t2 = csub(v[1], v[2]);
+	cplx<T> a = v[0];
+	v[0] = cadd(a, t1);
+	cplx<T> m1 = mk<T>(a.x + c * t1.x, a.y + c * t1.y);
+	cplx<T> m2 = mk<T>(-s * t2.y, s * t2.x); // i s t2
+	v[1] = cadd(m1, m2);
+	v[2] = csub(m1, m2);
+}
+
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft5(cplx<T>* v) {
+	const T c1 = (T)0.30901699437494742410229341718282;  // cos(2pi/5)
+	const T c2 = (T)-0.80901699437494742410229341718282; // cos(4pi/5)
+	const T s1 = (T)SIGN * (T)0.95105651629515357211643933337938; // sin(2pi/5)
+	const T s2 = (T)SIGN * (T)0.58778525229247312916870595463907; // sin(4pi/5)
+	cplx<T> a = v[0];
+	cplx<T> p1 = cadd(v[1], v[4]), m1 = csub(v[1], v[4]);
+	cplx<T> p2 = cadd(v[2], v[3]), m2 = csub(v[2], v[3]);
+	v[0] = cadd(a, cadd(p1, p2));
+	cplx<T> r1 = mk<T>(a.x + c1 * p1.x + c2 * p2.x, a.y + c1 * p1.y + c2 * p2.y);
+	cplx<T> r2 = mk<T>(a.x + c2 * p1.x + c1 * p2.x, a.y + c2 * p1.y + c1 * p2.y);
+	// i*(s1 m1 + s2 m2), i*(s2 m1 - s1 m2)
+	cplx<T> i1 = mk<T>(-(s1 * m1.y + s2 * m2.y), s1 * m1.x + s2 * m2.x);
+	cplx<T> i2 = mk<T>(-(s2 * m1.y - s1 * m2.y), s2 * m1.x - s1 * m2.x);
+	v[1] = cadd(r1, i1);
+	v[4] = csub(r1, i1);
+	v[2] = cadd(r2, i2);
+	v[3] = csub(r2, i2);
+}
+
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft7(cplx<T>* v) {
+	const T c1 = (T)0.62348980185873353052500488400424;   // cos(2pi/7)
+	const T c2 = (T)-0.22252093395631440428890256449680;  // cos(4pi/7)
+	const T c3 = (T)-0.90096886790241912623610231950745;  // cos(6pi/7)
+	const T s1 = (T)SIGN * (T)0.78183148246802980870844452667406; // sin(2pi/7)
+	const T s2 = (T)SIGN * (T)0.97492791218182360701813168299393; // sin(4pi/7)
+	const T s3 = (T)SIGN * (T)0.43388373911755812047576833284836; // sin(6pi/7)
+	cplx<T> a = v[0];
+	cplx<T> p1 = cadd(v[1], v[6]), m1 = csub(v[1], v[6]);
+	cplx<T> p2 = cadd(v[2], v[5]), m2 = csub(v[2], v[5]);
+	cplx<T> p3 = cadd(v[3], v[4]), m3 = csub(v[3], v[4]);
+	v[0] = cadd(a, cadd(p1, cadd(p2, p3)));
+	// k=1: c1 c2 c3 / s1 s2 s3 ; k=2: c2 c3(=cos 12pi/7 = c2? ) -> use cos(2pi*2r/7)
+	// cos(2pi*k*r/7) for r=1..3: k=1: c1,c2,c3 ; k=2: c2,c3,c1 ; k=3: c3,c1,c2
+	// sin(2pi*k*r/7):            k=1: s1,s2,s3 ; k=2: s2,-s3,-s1 ; k=3: s3,-s1,s2
+	cplx<T> r1 = mk<T>(a.x + c1 * p1.x + c2 * p2.x + c3 * p3.x, a.y + c1 * p1.y + c2 * p2.y + c3 * p3.y);
+	cplx<T> r2 = mk<T>(a.x + c2 * p1.x + c3 * p2.x + c1 * p3.x, a.y + c2 * p1.y + c3 * p2.y + c1 * p3.y);
+	cplx<T> r3 = mk<T>(a.x + c3 * p1.x + c1 * p2.x + c2 * p3.x, a.y + c3 * p1.y + c1 * p2.y + c2 * p3.y);
+	T j1x = s1 * m1.x + s2 * m2.x + s3 * m3.x, j1y = s1 * m1.y + s2 * m2.y + s3 * m3.y;
+	T j2x = s2 * m1.x - s3 * m2.x - s1 * m3.x, j2y = s2 * m1.y - s3 * m2.y - s1 * m3.y;
+	T j3x = s3 * m1.x - s1 * m2.x + s2 * m3.x, j3y = s3 * m1.y - s1 * m2.y + s2 * m3.y;
+	cplx<T> i1 = mk<T>(-j1y, j1x), i2 = mk<T>(-j2y, j2x), i3 = mk<T>(-j3y, j3x);
+	v[1] = cadd(r1, i1);
+	v[6] = csub(r1, i1);
+	v[2] = cadd(r2, i2);
+	v[5] = csub(r2, i2);
+	v[3] = cadd(r3, i3);
+	v[4] = csub(r3, i3);
+}
+
+template <int R, int SIGN, typename T> __host__ __device__ __forceinline__ void dft(cplx<T>* v) {
+	if constexpr (R == 2) dft2<SIGN, T>(v);
+	else if constexpr (R == 3) dft3<SIGN, T>(v);
+	else if constexpr (R == 4) dft4<SIGN, T>(v);
+	else if constexpr (R == 5) dft5<SIGN, T>(v);
+	else if constexpr (R == 7) dft7<SIGN, T>(v);
+	else if constexpr (R == 8) dft8<SIGN, T>(v);
+	else if constexpr (R == 16) dft16<SIGN, T>(v);
+}
+
+// ---------------------------------------------------------------- plans --
+
+// A transform length n = RMAIN^nmain * rtail * 3^n3 * 5^n5 * 7^n7 with
+// rtail in {1, 2, 4, 8} (< RMAIN), done as runs of one radix each: nmain
+// passes of RMAIN, one of rtail, then the odd radices. A loop body holding a
+// single radix keeps register allocation tight; the host fills the counts.
+struct FftPlan {
+	int n;
+	int nmain;
+	int rtail;
+	int n3, n5, n7;
+};
+
+// ---------------------------------------------------------------- passes -
+
+// One Stockham pass over P sequences (sequence p starts at buf + p*ld, padded
+// indexing inside a sequence). nthreads threads take part, thread index t.
+// Only the butterfly inputs are live across the barrier; twiddles are read
+// after it, so a thread needs about MAXE complex registers plus one DFT's
+// temporaries.
+template <int R, int SIGN, int MAXE, typename T>
+__device__ __forceinline__ void stockham_pass(cplx<T>* buf, int ld, int P, int n, int Ns,
+                                              const cplx<T>* __restrict__ tw, int t, int nthreads) {
+	constexpr int NB = MAXE / R;
+	static_assert(NB >= 1, "MAXE too small for radix");
+	const int nR = n / R;
+	const int total = P * nR;
+	cplx<T> v[NB][R];
+#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int b = t + i * nthreads;
+		if (b < total) {
+			const int p = b / nR;
+			const int j = b - p * nR;
+			const cplx<T>* in = buf + p * ld;
+#pragma unroll
+			for (int r = 0; r < R; r++) v[i][r] = in[pad<T>(j + r * nR)];
+		}
+	}
+	__syncthreads();
+	const int tstep = n / (Ns * R);
+#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int b = t + i * nthreads;
+		if (b < total) {
+			const int p = b / nR;
+			const int j = b - p * nR;
+			const int jm = j % Ns;
+			if (jm > 0) {
+				const cplx<T>* twj = tw + jm * tstep;
+#pragma unroll
+				for (int r = 1; r < R; r++) {
+					cplx<T> w = __ldg(twj + (r - 1) * jm * tstep);
+					if (SIGN > 0) w.y = -w.y;
+					v[i][r] = cmul(v[i][r], w);
+				}
+			}
+			dft<R, SIGN, T>(v[i]);
+			cplx<T>* out = buf + p * ld;
+			const int d0 = (j - jm) * R + jm;
+#pragma unroll
+			for (int r = 0; r < R; r++) out[pad<T>(d0 + r * Ns)] = v[i][r];
+		}
+	}
+	__syncthreads();
+}
+
+// Full transform of P sequences of length plan.n in place in shared memory.
+// RMAIN = MAXE; requires ceil(P * n / (R * nthreads)) <= MAXE / R for each radix R.
+template <int SIGN, int MAXE, typename T>
+__device__ __forceinline__ void fft_batch(cplx<T>* buf, int ld, int P, const FftPlan& plan,
+                                          const cplx<T>* __restrict__ tw, int t, int nthreads) {
+	constexpr int RM = MAXE;
+	const int n = plan.n;
+	int Ns = 1;
+	for (int s = 0; s < plan.nmain; s++) {
+		stockham_pass<RM, SIGN, MAXE, T>(buf, ld, P, n, Ns, tw, t, nthreads);
+		Ns *= RM;
+	}
+	if constexpr (RM > 8) {
+		if (plan.rtail == 8) { stockham_pass<8, SIGN, MAXE, T>(buf, ld, P, n, Ns, tw, t, nthreads); Ns *= 8; }
+	}
+	if (plan.rtail == 4) { stockham_pass<4, SIGN, MAXE, T>(buf, ld, P, n, Ns, tw, t, nthreads); Ns *= 4; }
+	else if (plan.rtail == 2) { stockham_pass<2, SIGN, MAXE, T>(buf, ld, P, n, Ns, tw, t, nthreads); Ns *= 2; }
+	for (int s = 0; s < plan.n3; s++) { stockham_pass<3, SIGN, MAXE, T>(buf, ld, P, n, Ns, tw, t, nthreads); Ns *= 3; }
+	for (int s = 0; s < plan.n5; s++) { stockham_pass<5, SIGN, MAXE, T>(buf, ld, P, n, Ns, tw, t, nthreads); Ns *= 5; }
+	for (int s = 0; s < plan.n7; s++) { stockham_pass<7, SIGN, MAXE, T>(buf, ld, P, n, Ns, tw, t, nthreads); Ns *= 7; }
+}
+
+// Transforms S resident sequences in sub-batches of at most SB (so that the
+// thread count needed by one fft_batch call stays within the CTA).
+template <int SIGN, int MAXE, typename T>
+__device__ __forceinline__ void fft_batches(cplx<T>* buf, int ld, int S, int SB, const FftPlan& plan,
+                                            const cplx<T>* __restrict__ tw, int t, int nthreads) {
+	for (int b0 = 0; b0 < S; b0 += SB) {
+		const int nb = (S - b0) < SB ? (S - b0) : SB;
+		fft_batch<SIGN, MAXE, T>(buf + b0 * ld, ld, nb, plan, tw, t, nthreads);
+	}
+}
+
+} // namespace pfcg

@@ -1,0 +1,122 @@
+// Kernel interfaces of the B200 relaxation path (implemented in kernels.cu).
+//
+// Data layout in HBM for a system of U fields on an Nx x Ny grid, H = Nx/2+1:
+//
+//   spec[u]  spectral state N^_u / (Nx Ny) without its k = 0 entry, complex,
+//            [kx][ky] with ky fastest (the reference's TRANSPOSED_OUT order,
+//            pfc-relax.c:227-228, index Ny*kx + ky). Entry (0,0) is kept 0.
+//   mean[u]  the k = 0 entry (the mean density), FP64.
+//   work[u]  the mixed (kx, y) representation between the two passes, complex,
+//            tiled by R rows: element (kx, y) at ((y/R)*H + kx)*R + y%R, so one
+//            row tile is contiguous for the x-pass and CC adjacent columns of
+//            one tile are contiguous for the y-pass.
+//
+// One time step is two kernels:
+//   x-pass (one CTA per R-row tile, all U fields): c2r along x of work,
+//     + mean -> real field m, nonlinear term NL(m) (pfc-relax.c:1188-1209),
+//     r2c along x -> work. Sum of NL (FP64) and a NaN flag are reduced on the way.
+//   y-pass (one CTA per CC columns, all U fields): forward FFT along y of work
+//     -> M^, k-space coupling and ETD1 update with A, B computed on the fly
+//     (pfc-relax.c:1215-1244, 901-958) against spec, write spec, inverse FFT
+//     along y -> work. The k = 0 entry is updated in FP64 from the NL sum, and
+//     the kx = 0 and kx = Nx/2 columns are projected onto their Hermitian part.
+// Pairs of real rows (or of fields) share one complex transform of length Nx.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fft_core.cuh"
+
+namespace pfcg {
+
+constexpr int MAXU = 4;
+constexpr int MAXW = 4;
+constexpr int MAX_CH = 8;     // real rows (channels) per x-pass CTA; odd counts pad with a zero channel
+constexpr int MAX_TRIAL = 5;  // box sizes per Parseval reduction
+
+struct Model {
+	int U;
+	int W[MAXU];
+	double c;  // 0 nonconserved, 1 conserved (normalised as pfc-relax.c:930)
+	double sigma, dt;
+	double lambda[MAXU], delta[MAXU];
+	double alpha[MAXU][MAXU], beta[MAXU][MAXU], gamma[MAXU][MAXU], epsilon[MAXU][MAXU], mu2[MAXU][MAXU];
+	double nu2[MAXU][MAXW], omega[MAXU][MAXW], phi[MAXU][MAXW];
+};
+
+struct Geom {
+	int Nx, Ny, H;
+	int R;      // rows per tile
+	int CC;     // columns per y-pass CTA
+	double dx, dy;
+};
+
+enum XMode { XP_STEP = 0, XP_EVAL = 1, XP_C2R = 2, XP_R2C = 3 };
+enum YMode { YP_STEP = 0, YP_INIT = 1, YP_WEIGHT = 2 };
+enum WKind { W_ONE = 0, W_P = 1, W_G = 2, W_Q = 3 };
+
+template <typename T> struct XArgs {
+	cplx<T>* work;          // U arrays at stride wstride
+	long long wstride;
+	const double* off;      // per-field value added after c2r / subtracted before r2c (the mean)
+	double* real;           // XP_C2R output / XP_R2C input: U fields of Ny*Nx doubles
+	double* acc;            // FP64 accumulators (see kernels.cu)
+	int* flag;              // NaN flag
+	const cplx<T>* tw;      // twiddles of length Nx
+	FftPlan plan;
+	int sb;                 // channel pairs per FFT call
+	Model m;
+	Geom g;
+};
+
+// Parameters of one k-space weight (YP_WEIGHT), resolved on the host so the
+// kernel never indexes the model by a runtime field index.
+struct WParams {
+	int W;
+	double nu2[MAXW], omega[MAXW], phi[MAXW];
+	double mu2;
+};
+
+template <typename T> struct YArgs {
+	cplx<T>* work;          // in/out (YP_STEP, YP_INIT) or out (YP_WEIGHT)
+	long long wstride;
+	cplx<T>* spec;          // U arrays at stride sstride
+	long long sstride;
+	double* mean;           // U, updated in place by YP_STEP at k = 0
+	double* acc;            // FP64 sum of NL per field (read and cleared by YP_STEP)
+	const cplx<T>* tw;      // twiddles of length Ny
+	FftPlan plan;
+	int sb;                 // sequences per FFT call
+	Model m;
+	Geom g;
+	int wkind, wsrc;        // YP_WEIGHT: weight kind and source field
+	WParams wp;             // YP_WEIGHT: parameters of the weight
+};
+
+struct LaunchCfg {
+	int grid, block, smem;
+};
+
+// Host-side launchers; return cudaGetLastError().
+template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
+template <typename T> cudaError_t launch_ypass(int mode, const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
+
+// Parseval sums for up to MAX_TRIAL box sizes (see kernels.cu): out[t] += ...
+template <typename T>
+cudaError_t launch_kspace_energy(const cplx<T>* spec, long long sstride, const Model& m, const Geom& g, int ntrial,
+                                 const double* dxs, const double* dys, double* out, cudaStream_t s);
+
+// Deterministic FP64 means of U real fields (npts each): per-block partial
+// sums into part[U * nblocks], then one block per field adds them in order.
+cudaError_t launch_field_means(const double* real, int U, long long npts, double* part, int nblocks, double* mean,
+                               cudaStream_t s);
+
+// f(r) assembly for write_energy: f = sum of local terms of m plus gradient /
+// smoothing couplings from the precomputed real fields (see kernels.cu).
+cudaError_t launch_energy_density(const double* m, const double* pn, const double* eta, const double* q, int npair,
+                                  const Model& mod, long long npts, double* f, cudaStream_t s);
+
+int max_elems_per_thread(bool fp64);
+int max_radix(bool fp64);
+
+} // namespace pfcg

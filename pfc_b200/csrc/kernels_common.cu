@@ -1,0 +1,89 @@
+// Precision-independent kernels and helpers of the B200 relaxation path.
+#include "kernels_impl.cuh"
+
+namespace pfcg {
+
+int max_elems_per_thread(bool fp64) { return fp64 ? FftCfg<double>::MAXE : FftCfg<float>::MAXE; }
+int max_radix(bool fp64) { return fp64 ? 8 : 16; }
+
+// ------------------------------------------------------ energy density --
+template <int U>
+__global__ void energy_density_kernel(const double* __restrict__ mf, const double* __restrict__ pn,
+                                      const double* __restrict__ eta, const double* __restrict__ q, const Model m,
+                                      long long npts, double* __restrict__ f) {
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npts; i += (long long)gridDim.x * blockDim.x) {
+		double fv = 0.0;
+		int pair = 0;
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const double nu = mf[u * npts + i], nunu = nu * nu;
+			fv += m.lambda[u] * nu + 0.5 * m.alpha[u][u] * nunu + 0.5 * m.beta[u][u] * nu * pn[u * npts + i] +
+			      (1.0 / 3.0) * m.gamma[u][u] * nu * nunu + 0.25 * m.delta[u] * nunu * nunu;
+#pragma unroll
+			for (int v = u + 1; v < U; v++, pair++) {
+				const double nv = mf[v * npts + i];
+				fv += m.alpha[u][v] * nu * nv + m.beta[u][v] * nu * q[pair * npts + i] +
+				      0.5 * m.gamma[u][v] * (nunu * nv + nu * nv * nv) + m.epsilon[u][v] * eta[u * npts + i] * eta[v * npts + i];
+			}
+		}
+		f[i] = fv;
+	}
+}
+
+cudaError_t launch_energy_density(const double* mf, const double* pn, const double* eta, const double* q, int npair,
+                                  const Model& mod, long long npts, double* f, cudaStream_t s) {
+	(void)npair;
+	int grid = (int)((npts + 255) / 256);
+	if (grid > 148 * 16) grid = 148 * 16;
+	switch (mod.U) {
+	case 1: energy_density_kernel<1><<<grid, 256, 0, s>>>(mf, pn, eta, q, mod, npts, f); break;
+	case 2: energy_density_kernel<2><<<grid, 256, 0, s>>>(mf, pn, eta, q, mod, npts, f); break;
+	case 3: energy_density_kernel<3><<<grid, 256, 0, s>>>(mf, pn, eta, q, mod, npts, f); break;
+	case 4: energy_density_kernel<4><<<grid, 256, 0, s>>>(mf, pn, eta, q, mod, npts, f); break;
+	default: return cudaErrorInvalidValue;
+	}
+	return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ field means --
+__global__ void __launch_bounds__(256) partial_sums_kernel(const double* __restrict__ real, long long npts,
+                                                            double* __restrict__ part) {
+	const int u = blockIdx.y;
+	const double* f = real + u * npts;
+	double s = 0.0;
+	for (long long i = blockIdx.x * 256LL + threadIdx.x; i < npts; i += (long long)gridDim.x * 256) s += f[i];
+	__shared__ double red[256];
+	red[threadIdx.x] = s;
+	__syncthreads();
+	for (int o = 128; o; o >>= 1) {
+		if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) part[u * gridDim.x + blockIdx.x] = red[0];
+}
+
+__global__ void __launch_bounds__(256) finish_means_kernel(const double* __restrict__ part, int nblocks, long long npts,
+                                                            double* __restrict__ mean) {
+	const int u = blockIdx.x;
+	double s = 0.0;
+	for (int i = threadIdx.x; i < nblocks; i += 256) s += part[u * nblocks + i];
+	__shared__ double red[256];
+	red[threadIdx.x] = s;
+	__syncthreads();
+	for (int o = 128; o; o >>= 1) {
+		if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) mean[u] = red[0] / (double)npts;
+}
+
+cudaError_t launch_field_means(const double* real, int U, long long npts, double* part, int nblocks, double* mean,
+                               cudaStream_t s) {
+	partial_sums_kernel<<<dim3(nblocks, U), 256, 0, s>>>(real, npts, part);
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) return e;
+	finish_means_kernel<<<U, 256, 0, s>>>(part, nblocks, npts, mean);
+	return cudaGetLastError();
+}
+
+} // namespace pfcg

@@ -1,0 +1,11 @@
+// F64 instantiation of the relaxation kernels (kernels_impl.cuh).
+#include "kernels_impl.cuh"
+
+namespace pfcg {
+
+template cudaError_t launch_xpass<double>(int, const XArgs<double>&, const LaunchCfg&, cudaStream_t);
+template cudaError_t launch_ypass<double>(int, const YArgs<double>&, const LaunchCfg&, cudaStream_t);
+template cudaError_t launch_kspace_energy<double>(const cplx<double>*, long long, const Model&, const Geom&, int, const double*,
+                                               const double*, double*, cudaStream_t);
+
+} // namespace pfcg

@@ -1,0 +1,625 @@
+// Kernels of the B200 relaxation path; see kernels.cuh for the data layout.
+// Included by kernels_f32.cu / kernels_f64.cu, which instantiate one precision
+// each, and by kernels_common.cu for the precision-independent parts.
+//
+// Reference correspondence (demos/honey/pfc-relax.c):
+//   xpass XP_STEP   nonlinear part in real space          :1188-1209
+//                   (c2r of :1246 and r2c of :1212 fused around it, x direction)
+//   ypass YP_STEP   k-space coupling + ETD1 update          :1215-1244
+//                   with A, B of update_AB                  :901-958
+//                   (y direction of the r2c :1212 and c2r :1246 fused around it)
+//   hermitian_column   spectral resynchronisation (in the y-pass) :1179-1185
+//   xpass XP_EVAL + kspace_energy   evaluate()              :988-1131
+//   energy_density  f(r) written by write_energy            :1094-1118, :817-859
+#pragma once
+
+#include <math.h>
+#include <stdio.h>
+
+#include "kernels.cuh"
+
+namespace pfcg {
+
+// Elements a thread holds during one FFT pass (and the largest radix):
+// 16 in FP32, 8 in FP64, so the butterfly inputs take 32 registers either way.
+template <typename T> struct FftCfg;
+template <> struct FftCfg<float> { static constexpr int MAXE = 16; };
+template <> struct FftCfg<double> { static constexpr int MAXE = 8; };
+constexpr int MAXNT = 512; // threads per CTA of the FFT kernels
+
+
+
+// --------------------------------------------------------------- helpers --
+
+template <int NV> __device__ __forceinline__ void block_reduce_add(double (&v)[NV], double* dst) {
+	__shared__ double red[32][NV > 0 ? NV : 1];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+	for (int i = 0; i < NV; i++)
+#pragma unroll
+		for (int o = 16; o; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+	if (lane == 0)
+#pragma unroll
+		for (int i = 0; i < NV; i++) red[warp][i] = v[i];
+	__syncthreads();
+	if (warp == 0) {
+#pragma unroll
+		for (int i = 0; i < NV; i++) {
+			double x = lane < nw ? red[lane][i] : 0.0;
+#pragma unroll
+			for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+			if (lane == 0) atomicAdd(dst + i, x);
+		}
+	}
+}
+
+template <typename T> __device__ __forceinline__ T expT(T x);
+template <> __device__ __forceinline__ float expT<float>(float x) { return expf(x); }
+template <> __device__ __forceinline__ double expT<double>(double x) { return exp(x); }
+
+// B = (exp(x) - 1)/a. FP64 follows pfc-relax.c:952 literally; FP32 uses expm1f,
+// which is the same quantity without the cancellation near a = 0.
+template <typename T> __device__ __forceinline__ T etd_b(T A, T x, T a);
+template <> __device__ __forceinline__ float etd_b<float>(float, float x, float a) { return expm1f(x) / a; }
+template <> __device__ __forceinline__ double etd_b<double>(double A, double, double a) { return (A - 1.0) / a; }
+
+// P_u(k^2) = prod_w (omega (nu2 - k2)^2 + phi), pfc-relax.c:943-947. Callers
+// pass a u that is a compile-time constant after unrolling, so nothing indexes
+// the parameter struct dynamically (that would copy it to local memory).
+template <typename T> __device__ __forceinline__ T P_of(const Model& m, int u, T k2) {
+	T P = (T)1;
+#pragma unroll
+	for (int w = 0; w < MAXW; w++) {
+		if (w < m.W[u]) {
+			T q = (T)m.nu2[u][w] - k2;
+			P *= (T)m.omega[u][w] * q * q + (T)m.phi[u][w];
+		}
+	}
+	return P;
+}
+
+__device__ __forceinline__ double k2_of(int kx, int ky, const Geom& g, double dx, double dy) {
+	const double dkx = 2.0 * 3.14159265358979323846264338327 / (dx * g.Nx);
+	const double dky = 2.0 * 3.14159265358979323846264338327 / (dy * g.Ny);
+	const double kxv = kx * dkx;
+	const double kyv = (ky < g.Ny / 2 ? ky : ky - g.Ny) * dky;
+	return kxv * kxv + kyv * kyv;
+}
+
+// ----------------------------------------------------------------- x-pass --
+
+template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 1) xpass_kernel(const XArgs<T> a) {
+	constexpr int MAXE = FftCfg<T>::MAXE;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
+	const int Nx = a.g.Nx, Ny = a.g.Ny, H = a.g.H, R = a.g.R;
+	const int CH = U * R;
+	const int P = (CH + 1) >> 1;
+	const int ld = padded_len<T>(Nx);
+	const int tile = blockIdx.x;
+	const int y0 = tile * R;
+	const int tid = threadIdx.x, nt = blockDim.x;
+	const long long tofs = (long long)tile * H * R;
+
+	double off[U];
+#pragma unroll
+	for (int u = 0; u < U; u++) off[u] = a.off ? a.off[u] : 0.0;
+
+	if constexpr (MODE == XP_R2C) {
+		// real rows (minus their mean) -> pairs of channels in one complex sequence
+		for (int x = tid; x < Nx; x += nt) {
+#pragma unroll
+			for (int p = 0; p < MAX_CH / 2; p++) {
+				if (p < P) {
+					const int c0 = 2 * p, c1 = 2 * p + 1;
+					const int u0 = c0 % U, r0 = c0 / U, u1 = c1 % U, r1 = c1 / U;
+					const double v0 = a.real[((long long)u0 * Ny + y0 + r0) * Nx + x] - (a.off ? a.off[u0] : 0.0);
+					const double v1 = (c1 < CH) ? a.real[((long long)u1 * Ny + y0 + r1) * Nx + x] - (a.off ? a.off[u1] : 0.0) : 0.0;
+					sm[p * ld + pad<T>(x)] = mk<T>((T)v0, (T)v1);
+				}
+			}
+		}
+	} else {
+		// Hermitian-extended spectra of channel pairs: C = A + iB on 0..Nx/2,
+		// conj(A) + i conj(B) on Nx/2+1..Nx-1; imaginary parts of the kx = 0 and
+		// kx = Nx/2 entries are dropped like a c2r transform does.
+		for (int k = tid; k < H; k += nt) {
+			cplx<T> y[MAX_CH];
+#pragma unroll
+			for (int c = 0; c < MAX_CH; c++) {
+				y[c] = mk<T>((T)0, (T)0);
+				if (c < CH) {
+					const int u = c % U, r = c / U;
+					y[c] = a.work[u * a.wstride + tofs + (long long)k * R + r];
+				}
+			}
+			const bool selfc = (k == 0) || (2 * k == Nx);
+#pragma unroll
+			for (int p = 0; p < MAX_CH / 2; p++) {
+				if (p < P) {
+					cplx<T> A = y[2 * p], B = y[2 * p + 1];
+					if (selfc) { A.y = (T)0; B.y = (T)0; }
+					sm[p * ld + pad<T>(k)] = mk<T>(A.x - B.y, A.y + B.x);
+					if (k > 0 && 2 * k < Nx) sm[p * ld + pad<T>(Nx - k)] = mk<T>(A.x + B.y, B.x - A.y);
+				}
+			}
+		}
+		__syncthreads();
+		fft_batches<+1, MAXE, T>(sm, ld, P, a.sb, a.plan, a.tw, tid, nt);
+	}
+
+	if constexpr (MODE == XP_STEP || MODE == XP_EVAL || MODE == XP_C2R) {
+		constexpr int NACC = (MODE == XP_EVAL) ? 1 + U : U;
+		double acc[NACC];
+#pragma unroll
+		for (int i = 0; i < NACC; i++) acc[i] = 0.0;
+		bool nan = false;
+		T lam[U], del[U], gam[U][U], alp[U][U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			lam[u] = (T)a.m.lambda[u];
+			del[u] = (T)a.m.delta[u];
+#pragma unroll
+			for (int v = 0; v < U; v++) { gam[u][v] = (T)a.m.gamma[u][v]; alp[u][v] = (T)a.m.alpha[u][v]; }
+		}
+		for (int x = tid; x < Nx; x += nt) {
+			T z[MAX_CH];
+#pragma unroll
+			for (int p = 0; p < MAX_CH / 2; p++) {
+				if (p < P) {
+					const cplx<T> v = sm[p * ld + pad<T>(x)];
+					z[2 * p] = v.x;
+					z[2 * p + 1] = v.y;
+				}
+			}
+#pragma unroll
+			for (int r = 0; r < MAX_CH / U; r++) {
+				if (r < R) {
+					if constexpr (MODE == XP_STEP) {
+						T mv[U], mc[U];
+#pragma unroll
+						for (int u = 0; u < U; u++) {
+							mv[u] = z[r * U + u] + (T)off[u];
+							nan |= (mv[u] != mv[u]);
+							mc[u] = (T)0;
+						}
+#pragma unroll
+						for (int u = 0; u < U - 1; u++)
+#pragma unroll
+							for (int v = u + 1; v < U; v++) {
+								mc[u] += alp[u][v] * mv[v] + (T)0.5 * gam[u][v] * ((T)2 * mv[u] * mv[v] + mv[v] * mv[v]);
+								mc[v] += alp[u][v] * mv[u] + (T)0.5 * gam[u][v] * ((T)2 * mv[v] * mv[u] + mv[u] * mv[u]);
+							}
+#pragma unroll
+						for (int u = 0; u < U; u++) {
+							const T m2 = mv[u] * mv[u];
+							const T nl = lam[u] + gam[u][u] * m2 + del[u] * mv[u] * m2 + mc[u];
+							z[r * U + u] = nl;
+							acc[u] += (double)nl;
+						}
+					} else if constexpr (MODE == XP_EVAL) {
+						double mv[U];
+#pragma unroll
+						for (int u = 0; u < U; u++) mv[u] = (double)z[r * U + u] + off[u];
+						double f = 0.0;
+#pragma unroll
+						for (int u = 0; u < U; u++) {
+							const double n1 = mv[u], n2 = n1 * n1;
+							f += a.m.lambda[u] * n1 + 0.5 * a.m.alpha[u][u] * n2 + (1.0 / 3.0) * a.m.gamma[u][u] * n1 * n2 +
+							     0.25 * a.m.delta[u] * n2 * n2;
+#pragma unroll
+							for (int v = u + 1; v < U; v++) {
+								const double nv = mv[v];
+								f += a.m.alpha[u][v] * n1 * nv + 0.5 * a.m.gamma[u][v] * (n2 * nv + n1 * nv * nv);
+							}
+							acc[1 + u] += n1;
+						}
+						acc[0] += f;
+					} else {
+#pragma unroll
+						for (int u = 0; u < U; u++)
+							a.real[((long long)u * Ny + y0 + r) * Nx + x] = (double)z[r * U + u] + off[u];
+					}
+				}
+			}
+			if constexpr (MODE == XP_STEP) {
+#pragma unroll
+				for (int p = 0; p < MAX_CH / 2; p++)
+					if (p < P) sm[p * ld + pad<T>(x)] = mk<T>(z[2 * p], (2 * p + 1 < CH) ? z[2 * p + 1] : (T)0);
+			}
+		}
+		if constexpr (MODE == XP_STEP) {
+			if (nan) atomicOr(a.flag, 1);
+			block_reduce_add<NACC>(acc, a.acc);
+		} else if constexpr (MODE == XP_EVAL) {
+			block_reduce_add<NACC>(acc, a.acc);
+		}
+	}
+
+	if constexpr (MODE == XP_STEP || MODE == XP_R2C) {
+		__syncthreads();
+		fft_batches<-1, MAXE, T>(sm, ld, P, a.sb, a.plan, a.tw, tid, nt);
+		// split each pair: Za = (C[k] + conj C[-k]) / 2, Zb = (C[k] - conj C[-k]) / (2i)
+		const T half = (T)0.5;
+		for (int k = tid; k < H; k += nt) {
+			const int km = (k == 0) ? 0 : Nx - k;
+			cplx<T> zz[MAX_CH];
+#pragma unroll
+			for (int p = 0; p < MAX_CH / 2; p++) {
+				if (p < P) {
+					const cplx<T> Ck = sm[p * ld + pad<T>(k)];
+					const cplx<T> Cm = sm[p * ld + pad<T>(km)];
+					zz[2 * p] = mk<T>(half * (Ck.x + Cm.x), half * (Ck.y - Cm.y));
+					zz[2 * p + 1] = mk<T>(half * (Ck.y + Cm.y), half * (Cm.x - Ck.x));
+				}
+			}
+#pragma unroll
+			for (int c = 0; c < MAX_CH; c++) {
+				if (c < CH) {
+					const int u = c % U, r = c / U;
+					a.work[u * a.wstride + tofs + (long long)k * R + r] = zz[c];
+				}
+			}
+		}
+	}
+}
+
+// ----------------------------------------------------------------- y-pass --
+
+// Hermitian projection of one resident column (kx = 0 or kx = Nx/2): entry ky
+// and entry Ny - ky become (a + conj b)/2 and its conjugate, self-conjugate
+// entries become real. Writes shared memory and the spectral state. This is
+// the reference's resynchronisation N^ = FFT(c2r(N^)) (pfc-relax.c:1179-1185)
+// restricted to the only columns where it is not the identity, done every
+// step: their anti-Hermitian part is invisible to c2r and is not acted on by
+// the nonlinear term, so between resyncs it grows like A(k)^t for every
+// unstable k (x1.28 per step for epsilon = -0.25, dt = 1), which overflows in FP32.
+template <typename T>
+__device__ __forceinline__ void hermitian_column(cplx<T>* col, cplx<T>* spec_col, int Ny, int tid, int nt) {
+	const int half = Ny / 2;
+	for (int base = 0; base <= half; base += nt) {
+		const int j = base + tid;
+		cplx<T> p = mk<T>((T)0, (T)0);
+		const int jn = (Ny - j) % Ny;
+		if (j <= half) {
+			const cplx<T> a = col[pad<T>(j)], b = col[pad<T>(jn)];
+			p = mk<T>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y));
+		}
+		__syncthreads();
+		if (j <= half) {
+			col[pad<T>(j)] = p;
+			spec_col[j] = p;
+			if (jn != j) {
+				col[pad<T>(jn)] = cconj(p);
+				spec_col[jn] = cconj(p);
+			}
+		}
+		__syncthreads();
+	}
+}
+
+template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 1) ypass_kernel(const YArgs<T> a) {
+	constexpr int MAXE = FftCfg<T>::MAXE;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
+	const int Nx = a.g.Nx, Ny = a.g.Ny, H = a.g.H, R = a.g.R, CC = a.g.CC;
+	const int S = U * CC;
+	const int ld = padded_len<T>(Ny);
+	const int kx0 = blockIdx.x * CC;
+	const int ncol = min(CC, H - kx0);
+	const int ntile = Ny / R;
+	const long long tileH = (long long)H * R;
+	const int chunk = CC * R;
+	const int tid = threadIdx.x, nt = blockDim.x;
+
+	if constexpr (MODE != YP_WEIGHT) {
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const cplx<T>* src = a.work + u * a.wstride + (long long)kx0 * R;
+			for (int e = tid; e < ntile * chunk; e += nt) {
+				const int t = e / chunk, rem = e - t * chunk;
+				const int c = rem / R, r = rem - c * R;
+				cplx<T> v = mk<T>((T)0, (T)0);
+				if (c < ncol) v = src[t * tileH + rem];
+				sm[(u * CC + c) * ld + pad<T>(t * R + r)] = v;
+			}
+		}
+		__syncthreads();
+		fft_batches<-1, MAXE, T>(sm, ld, S, a.sb, a.plan, a.tw, tid, nt);
+	}
+
+	const double dx = a.g.dx, dy = a.g.dy;
+	if constexpr (MODE == YP_STEP) {
+		const T invN = (T)(1.0 / ((double)Nx * (double)Ny));
+		const T cc = (T)a.m.c;
+		const T dt = (T)a.m.dt;
+		const double ag = -0.5 / a.m.sigma / a.m.sigma;
+		for (int e = tid; e < CC * Ny; e += nt) {
+			const int c = e / Ny, ky = e - c * Ny;
+			if (c >= ncol) continue;
+			const int kx = kx0 + c;
+			const T k2 = (T)k2_of(kx, ky, a.g, dx, dy);
+			const long long si = (long long)kx * Ny + ky;
+			cplx<T> Nv[U], Mv[U];
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				Nv[u] = a.spec[u * a.sstride + si];
+				Mv[u] = cscale(sm[(u * CC + c) * ld + pad<T>(ky)], invN);
+			}
+			if constexpr (U > 1) {
+				T G = expT<T>((T)ag * k2);
+				const T G2 = G * G;
+#pragma unroll
+				for (int u = 0; u < U - 1; u++)
+#pragma unroll
+					for (int v = u + 1; v < U; v++) {
+						T d2 = (T)a.m.mu2[u][v] - k2;
+						d2 *= d2;
+						const T cu = (T)a.m.beta[u][v] * d2 + (T)a.m.epsilon[u][v] * G2;
+						Mv[u] = cadd(Mv[u], cscale(Nv[v], cu));
+						Mv[v] = cadd(Mv[v], cscale(Nv[u], cu));
+					}
+			}
+			const bool origin = (kx == 0 && ky == 0);
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				const T av = (T)a.m.alpha[u][u] + (T)a.m.beta[u][u] * P_of<T>(a.m, u, k2);
+				const T o = cc - (T)1 - cc * k2;
+				const T x = o * av * dt;
+				const T A = expT<T>(x);
+				const T Bn = (av == (T)0) ? o * dt : etd_b<T>(A, x, av);
+				cplx<T> nn = cadd(cscale(Nv[u], A), cscale(Mv[u], Bn));
+				if (origin) nn = mk<T>((T)0, (T)0);
+				a.spec[u * a.sstride + si] = nn;
+				sm[(u * CC + c) * ld + pad<T>(ky)] = nn;
+			}
+		}
+		if (kx0 == 0 && tid == 0) {
+			// k = 0 in FP64: mean' = A(0) mean + B(0) (sum NL + couplings), pfc-relax.c:1215-1244 at k = 0
+			const double NxNy = (double)Nx * (double)Ny;
+			double mean0[U], Mk[U];
+#pragma unroll
+			for (int u = 0; u < U; u++) { mean0[u] = a.mean[u]; Mk[u] = a.acc[u]; }
+#pragma unroll
+			for (int u = 0; u < U - 1; u++)
+#pragma unroll
+				for (int v = u + 1; v < U; v++) {
+					const double d2 = a.m.mu2[u][v] * a.m.mu2[u][v];
+					const double cu = a.m.beta[u][v] * d2 + a.m.epsilon[u][v];
+					Mk[u] += cu * mean0[v] * NxNy;
+					Mk[v] += cu * mean0[u] * NxNy;
+				}
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				const double P0 = P_of<double>(a.m, u, 0.0);
+				const double av = a.m.alpha[u][u] + a.m.beta[u][u] * P0;
+				const double o = a.m.c - 1.0;
+				const double A = exp(o * av * a.m.dt);
+				const double B = ((av == 0.0) ? o * a.m.dt : (A - 1.0) / av) / NxNy;
+				a.mean[u] = A * mean0[u] + B * Mk[u];
+				a.acc[u] = 0.0;
+			}
+		}
+	} else if constexpr (MODE == YP_INIT) {
+		const T invN = (T)(1.0 / ((double)Nx * (double)Ny));
+		for (int e = tid; e < CC * Ny; e += nt) {
+			const int c = e / Ny, ky = e - c * Ny;
+			if (c >= ncol) continue;
+			const int kx = kx0 + c;
+			const long long si = (long long)kx * Ny + ky;
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				cplx<T> nn = cscale(sm[(u * CC + c) * ld + pad<T>(ky)], invN);
+				if (kx == 0 && ky == 0) nn = mk<T>((T)0, (T)0);
+				a.spec[u * a.sstride + si] = nn;
+				sm[(u * CC + c) * ld + pad<T>(ky)] = nn;
+			}
+		}
+	} else {
+		// YP_WEIGHT (U == 1): w(k) * spec[src] -> sm, with the weight's
+		// parameters in a.wp (field index resolved on the host)
+		const double ag = -0.5 / a.m.sigma / a.m.sigma;
+		const cplx<T>* src = a.spec + a.wsrc * a.sstride;
+		for (int e = tid; e < CC * Ny; e += nt) {
+			const int c = e / Ny, ky = e - c * Ny;
+			const int kx = kx0 + c;
+			cplx<T> nn = mk<T>((T)0, (T)0);
+			if (c < ncol && !(kx == 0 && ky == 0)) {
+				const double k2 = k2_of(kx, ky, a.g, dx, dy);
+				double w = 1.0;
+				if (a.wkind == W_P) {
+#pragma unroll
+					for (int q = 0; q < MAXW; q++)
+						if (q < a.wp.W) {
+							const double d = a.wp.nu2[q] - k2;
+							w *= a.wp.omega[q] * d * d + a.wp.phi[q];
+						}
+				} else if (a.wkind == W_G) {
+					w = exp(ag * k2);
+				} else if (a.wkind == W_Q) {
+					const double d = a.wp.mu2 - k2;
+					w = d * d;
+				}
+				nn = cscale(src[(long long)kx * Ny + ky], (T)w);
+			}
+			sm[c * ld + pad<T>(ky)] = nn;
+		}
+	}
+
+	if constexpr (MODE == YP_STEP || MODE == YP_INIT) {
+		// kx = 0 and (even Nx) kx = Nx/2 columns: keep them exactly Hermitian
+		const bool has0 = (kx0 == 0);
+		const int kn = (Nx % 2 == 0) ? Nx / 2 : -1;
+		const bool hasn = (kn >= kx0 && kn < kx0 + ncol);
+		if (has0 || hasn) {
+			__syncthreads();
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				if (has0) hermitian_column<T>(sm + (u * CC) * ld, a.spec + u * a.sstride, Ny, tid, nt);
+				if (hasn)
+					hermitian_column<T>(sm + (u * CC + (kn - kx0)) * ld, a.spec + u * a.sstride + (long long)kn * Ny, Ny,
+					                    tid, nt);
+			}
+		}
+	}
+	__syncthreads();
+	fft_batches<+1, MAXE, T>(sm, ld, S, a.sb, a.plan, a.tw, tid, nt);
+
+#pragma unroll
+	for (int u = 0; u < U; u++) {
+		cplx<T>* dst = a.work + u * a.wstride + (long long)kx0 * R;
+		for (int e = tid; e < ntile * chunk; e += nt) {
+			const int t = e / chunk, rem = e - t * chunk;
+			const int c = rem / R, r = rem - c * R;
+			if (c < ncol) dst[t * tileH + rem] = sm[(u * CC + c) * ld + pad<T>(t * R + r)];
+		}
+	}
+}
+
+// ------------------------------------------------------- Parseval energy --
+// <f> gradient/coupling part in k space, for several box sizes at once:
+//   sum over the half spectrum with weight 1 (kx = 0, Nx/2) or 2 of
+//   1/2 beta_uu P_u |N_u|^2 + sum_{u<v} (beta_uv (mu2_uv - k2)^2 + eps_uv G^2) Re(N_u conj N_v),
+// which equals the mean over the grid of the beta and epsilon terms of
+// pfc-relax.c:1101-1111 (Parseval; N^ normalised by 1/(Nx Ny)).
+struct Trials {
+	double dx[MAX_TRIAL], dy[MAX_TRIAL];
+};
+
+template <typename T, int U>
+__global__ void __launch_bounds__(256) kspace_energy_kernel(const cplx<T>* __restrict__ spec, long long sstride, const Model m,
+                                                           const Geom g, int ntrial, const Trials tr, double* out) {
+	double acc[MAX_TRIAL];
+#pragma unroll
+	for (int t = 0; t < MAX_TRIAL; t++) acc[t] = 0.0;
+	const long long total = (long long)g.H * g.Ny;
+	const double ag = -1.0 / m.sigma / m.sigma; // G^2 = exp(-k2 / sigma^2)
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+		const int kx = (int)(i / g.Ny), ky = (int)(i - (long long)kx * g.Ny);
+		const double wgt = (kx == 0 || 2 * kx == g.Nx) ? 1.0 : 2.0;
+		double nr[U], ni[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const cplx<T> v = spec[u * sstride + i];
+			nr[u] = (double)v.x;
+			ni[u] = (double)v.y;
+		}
+#pragma unroll
+		for (int t = 0; t < MAX_TRIAL; t++) {
+			if (t < ntrial) {
+				const double k2 = k2_of(kx, ky, g, tr.dx[t], tr.dy[t]);
+				double e = 0.0;
+#pragma unroll
+				for (int u = 0; u < U; u++) e += 0.5 * m.beta[u][u] * P_of<double>(m, u, k2) * (nr[u] * nr[u] + ni[u] * ni[u]);
+				if constexpr (U > 1) {
+					const double G2 = exp(ag * k2);
+#pragma unroll
+					for (int u = 0; u < U - 1; u++)
+#pragma unroll
+						for (int v = u + 1; v < U; v++) {
+							const double d = m.mu2[u][v] - k2;
+							e += (m.beta[u][v] * d * d + m.epsilon[u][v] * G2) * (nr[u] * nr[v] + ni[u] * ni[v]);
+						}
+				}
+				acc[t] += wgt * e;
+			}
+		}
+	}
+	block_reduce_add<MAX_TRIAL>(acc, out);
+}
+
+// -------------------------------------------------------------- launchers --
+
+// Raises the dynamic shared-memory limit of a kernel once per device.
+template <typename K> static void smem_attr(K k, unsigned long long& mask) {
+	int dev = 0;
+	cudaGetDevice(&dev);
+	const unsigned long long bit = 1ull << (dev & 63);
+	if (!(mask & bit)) {
+		cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+		mask |= bit;
+	}
+}
+
+template <typename T, int U, int MODE> static cudaError_t xlaunch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	auto k = xpass_kernel<T, U, MODE>;
+	static unsigned long long mask = 0;
+	smem_attr(k, mask);
+	k<<<c.grid, c.block, c.smem, s>>>(a);
+	return cudaGetLastError();
+}
+
+template <typename T, int U> static cudaError_t xlaunch_mode(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	switch (mode) {
+	case XP_STEP: return xlaunch<T, U, XP_STEP>(a, c, s);
+	case XP_EVAL: return xlaunch<T, U, XP_EVAL>(a, c, s);
+	case XP_C2R: return xlaunch<T, U, XP_C2R>(a, c, s);
+	case XP_R2C: return xlaunch<T, U, XP_R2C>(a, c, s);
+	}
+	return cudaErrorInvalidValue;
+}
+
+template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	switch (a.m.U) {
+	case 1: return xlaunch_mode<T, 1>(mode, a, c, s);
+	case 2: return xlaunch_mode<T, 2>(mode, a, c, s);
+	case 3: return xlaunch_mode<T, 3>(mode, a, c, s);
+	case 4: return xlaunch_mode<T, 4>(mode, a, c, s);
+	}
+	return cudaErrorInvalidValue;
+}
+
+template <typename T, int U, int MODE> static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	auto k = ypass_kernel<T, U, MODE>;
+	static unsigned long long mask = 0;
+	smem_attr(k, mask);
+	k<<<c.grid, c.block, c.smem, s>>>(a);
+	return cudaGetLastError();
+}
+
+template <typename T> cudaError_t launch_ypass(int mode, const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	if (mode == YP_WEIGHT) return ylaunch<T, 1, YP_WEIGHT>(a, c, s);
+	if (mode == YP_STEP) {
+		switch (a.m.U) {
+		case 1: return ylaunch<T, 1, YP_STEP>(a, c, s);
+		case 2: return ylaunch<T, 2, YP_STEP>(a, c, s);
+		case 3: return ylaunch<T, 3, YP_STEP>(a, c, s);
+		case 4: return ylaunch<T, 4, YP_STEP>(a, c, s);
+		}
+	}
+	if (mode == YP_INIT) {
+		switch (a.m.U) {
+		case 1: return ylaunch<T, 1, YP_INIT>(a, c, s);
+		case 2: return ylaunch<T, 2, YP_INIT>(a, c, s);
+		case 3: return ylaunch<T, 3, YP_INIT>(a, c, s);
+		case 4: return ylaunch<T, 4, YP_INIT>(a, c, s);
+		}
+	}
+	return cudaErrorInvalidValue;
+}
+
+
+template <typename T>
+cudaError_t launch_kspace_energy(const cplx<T>* spec, long long sstride, const Model& m, const Geom& g, int ntrial,
+                                 const double* dxs, const double* dys, double* out, cudaStream_t s) {
+	Trials tr;
+	for (int t = 0; t < MAX_TRIAL; t++) {
+		tr.dx[t] = t < ntrial ? dxs[t] : 1.0;
+		tr.dy[t] = t < ntrial ? dys[t] : 1.0;
+	}
+	const long long total = (long long)g.H * g.Ny;
+	int grid = (int)((total + 255) / 256);
+	if (grid > 148 * 8) grid = 148 * 8;
+	switch (m.U) {
+	case 1: kspace_energy_kernel<T, 1><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
+	case 2: kspace_energy_kernel<T, 2><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
+	case 3: kspace_energy_kernel<T, 3><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
+	case 4: kspace_energy_kernel<T, 4><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
+	default: return cudaErrorInvalidValue;
+	}
+	return cudaGetLastError();
+}
+
+
+} // namespace pfcg

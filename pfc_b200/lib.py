@@ -1,0 +1,223 @@
+"""ctypes view of libpfc_b200.so (the C ABI in include/pfc_b200.h).
+
+The shared library is built in-tree (``make -C pfc_b200``). There is no CPU
+fallback: if the library or a CUDA device is missing, every entry point
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import Params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpfc_b200.so")
+DRIVER_PATH = os.path.join(HERE, "pfc-relax")
+
+FP32, FP64 = 0, 1
+
+OK = 0
+NAN = 39
+EARG, ECUDA, ESIZE, ENOMEM, ETIMEOUT, ENODEV = -1, -2, -3, -4, -5, -6
+
+# every entry point of include/pfc_b200.h with its ctypes signature
+_vp, _ip, _dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "pfcg_size_supported": (ctypes.c_int, [_ip, _ip]),
+    "pfcg_create": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_double, ctypes.c_double, _ip,
+                                   ctypes.POINTER(ctypes.c_void_p)]),
+    "pfcg_upload": (ctypes.c_int, [_vp, _dp]),
+    "pfcg_download": (ctypes.c_int, [_vp, _dp]),
+    "pfcg_set_box": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
+    "pfcg_get_box": (ctypes.c_int, [_vp, _dp, _dp]),
+    "pfcg_set_time": (ctypes.c_int, [_vp, _ip]),
+    "pfcg_get_time": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
+    "pfcg_step": (ctypes.c_int, [_vp, _ip]),
+    "pfcg_evaluate": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+    "pfcg_optimize": (ctypes.c_int, [_vp, _ip, _ip, _dp]),
+    "pfcg_set_device": (ctypes.c_int, [_ip]),
+    "pfcg_set_profiling": (ctypes.c_int, [_vp, _ip]),
+    "pfcg_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _ip]),
+    "pfcg_stream": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
+    "pfcg_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "pfcg_last_error": (ctypes.c_char_p, [_vp]),
+    "pfcg_destroy": (None, [_vp]),
+}
+
+_lib = None
+
+
+class PfcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("pfcg error %d: %s" % (code, msg))
+        self.code = code
+
+
+def load():
+    """Loads libpfc_b200.so once; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libpfc_b200.so is not built (run `make -C pfc_b200`); there is no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def size_supported(Nx: int, Ny: int) -> bool:
+    return bool(load().pfcg_size_supported(Nx, Ny))
+
+
+def set_device(device: int) -> None:
+    """Device that later Relaxation objects on this thread use."""
+    L = load()
+    rc = L.pfcg_set_device(device)
+    if rc:
+        raise PfcError(rc, L.pfcg_last_error(None).decode())
+
+
+class Relaxation:
+    """One relaxation on the GPU: the state of pfc-relax's struct S for the hot
+    path (fields, spectral state, box size, step counter)."""
+
+    def __init__(self, params: Params, Nx: int, Ny: int, dx: float, dy: float, precision: str = "fp64"):
+        self.L = load()
+        self.params = params
+        self.U = params.U
+        self.Nx, self.Ny = Nx, Ny
+        self.precision = precision
+        prec = {"fp32": FP32, "fp64": FP64}[precision]
+        h = ctypes.c_void_p()
+        rc = self.L.pfcg_create(ctypes.byref(params), Nx, Ny, dx, dy, prec, ctypes.byref(h))
+        if rc:
+            raise PfcError(rc, self.L.pfcg_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc: int):
+        if rc:
+            raise PfcError(rc, self.L.pfcg_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pfcg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def upload(self, fields: np.ndarray) -> None:
+        f = np.ascontiguousarray(fields, dtype=np.float64).reshape(self.U, self.Ny, self.Nx)
+        self._check(self.L.pfcg_upload(self.h, _dptr(f)))
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.U, self.Ny, self.Nx))
+        self._check(self.L.pfcg_download(self.h, _dptr(out)))
+        return out
+
+    def step(self, n: int = 1) -> int:
+        """Advances n steps; returns 0, or raises PfcError (code 39 for NaN)."""
+        rc = self.L.pfcg_step(self.h, n)
+        self._check(rc)
+        return rc
+
+    def step_rc(self, n: int = 1) -> int:
+        """Like step() but returns the status code instead of raising."""
+        return self.L.pfcg_step(self.h, n)
+
+    def evaluate(self, want_f: bool = False):
+        fave = ctypes.c_double()
+        nave = np.zeros(self.U)
+        f = np.empty((self.Ny, self.Nx)) if want_f else None
+        self._check(self.L.pfcg_evaluate(self.h, ctypes.byref(fave), _dptr(nave), _dptr(f) if want_f else None))
+        return (fave.value, nave, f) if want_f else (fave.value, nave)
+
+    def optimize(self, xopt: int, yopt: int, d: float) -> float:
+        dd = ctypes.c_double(d)
+        self._check(self.L.pfcg_optimize(self.h, xopt, yopt, ctypes.byref(dd)))
+        return dd.value
+
+    def set_box(self, dx: float, dy: float) -> None:
+        self._check(self.L.pfcg_set_box(self.h, dx, dy))
+
+    def box(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.pfcg_get_box(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    @property
+    def t(self) -> int:
+        v = ctypes.c_int()
+        self._check(self.L.pfcg_get_time(self.h, ctypes.byref(v)))
+        return v.value
+
+    def set_time(self, t: int) -> None:
+        self._check(self.L.pfcg_set_time(self.h, t))
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.L.pfcg_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def set_profiling(self, on: bool) -> None:
+        self._check(self.L.pfcg_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self):
+        """{kind: (ms, launches)} for kinds 'xpass', 'ypass', 'other' since profiling was switched on."""
+        ms = np.zeros(3)
+        n = (ctypes.c_longlong * 3)()
+        self._check(self.L.pfcg_profile_read(self.h, _dptr(ms), n, 3))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(("xpass", "ypass", "other"))}
+
+    @property
+    def launches(self) -> int:
+        c = ctypes.c_longlong()
+        self._check(self.L.pfcg_launch_count(self.h, ctypes.byref(c)))
+        return c.value
+
+    def relax(self, tend: int, Tprint: int, Topt: int = 0, xopt: int = 1, yopt: int = 1, on_print=None):
+        """pfc-relax.c:1293-1313 relax() schedule without file output, stepping
+        in chunks between events. Returns the printed rows (t, dx, dy, <f>, <n_u>...)."""
+        rows = []
+        d = 1e-4
+        t = self.t
+        while t <= tend:
+            if Topt > 0 and t > 0 and t % Topt == 0:
+                d = self.optimize(xopt, yopt, d)
+            if t % Tprint == 0:
+                fave, nave = self.evaluate()
+                dx, dy = self.box()
+                row = [t, dx, dy, fave] + list(nave)
+                rows.append(row)
+                if on_print:
+                    on_print(row)
+            if t >= tend:
+                break
+            nxt = tend
+            for T in (Tprint, Topt):
+                if T > 0:
+                    nxt = min(nxt, (t // T + 1) * T)
+            self.step(nxt - t)
+            t = nxt
+        return np.array(rows)
