@@ -13,6 +13,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -58,6 +59,9 @@ struct pfcg_handle {
 	double* h_buf = nullptr; // pinned: ACC_N accumulators, MAXU means, OFFS_N offsets
 	FftPlan px{}, py{};
 	LaunchCfg cx{}, cy{}, cx1{}, cy1{};
+	LaunchCfg cxs{}, cys{}; // STEP kernels (possibly compile-time specialised)
+	void* twctx = nullptr;  // per-pass twiddle tables of the specialised kernels
+	void* twcty = nullptr;
 	int sbx = 1, sby = 1, sbx1 = 1, sby1 = 1;
 	double* d_real = nullptr;   // U*Ny*Nx doubles
 	double* d_fields = nullptr; // f(r) work fields
@@ -73,6 +77,12 @@ struct pfcg_handle {
 };
 
 namespace {
+
+// wave-number steps of the current box, pfc-relax.c:916-917
+void set_dk(pfcg_handle* h) {
+	h->geom.dkx = 2.0 * PI / (h->geom.dx * h->Nx);
+	h->geom.dky = 2.0 * PI / (h->geom.dy * h->Ny);
+}
 
 int fail(pfcg_handle* h, int code, const std::string& msg) {
 	if (h) h->err = msg;
@@ -152,7 +162,14 @@ int choose_layout(pfcg_handle* h, int nsm) {
 	const int want = 2 * nsm;
 	const int U = h->U;
 	int R = 0;
+	// the compile-time specialised STEP kernels fix the tile shape when the size has one
+	// PFCG_GENERIC_KERNELS=1 in the environment disables them (A/B checks)
+	const char* gen = std::getenv("PFCG_GENERIC_KERNELS");
+	const bool allow_spec = !(gen && gen[0] == '1');
+	const int rs = allow_spec ? spec_rows(fp64, U, h->Nx) : 0;
+	if (rs && h->Ny % rs == 0) R = rs;
 	for (int r : {8, 4, 2, 1}) {
+		if (R) break;
 		if (h->Ny % r) continue;
 		const int CH = U * r;
 		if (CH > MAX_CH) continue;
@@ -165,7 +182,10 @@ int choose_layout(pfcg_handle* h, int nsm) {
 	}
 	if (!R) return fail(h, PFCG_ESIZE, "no x-pass tile fits shared memory for this Nx");
 	int CC = 0;
+	const bool yspec = allow_spec && spec_cols(fp64, U, h->Ny) && spec_rows(fp64, U, h->Ny) == R;
+	if (yspec) CC = spec_cols(fp64, U, h->Ny);
 	for (int c : {4, 2, 1}) {
+		if (CC) break;
 		const int S = U * c;
 		if ((size_t)S * padded(h->Ny, fp64) * h->celem > budget) continue;
 		int nt;
@@ -189,6 +209,42 @@ int choose_layout(pfcg_handle* h, int nsm) {
 	h->cy = {(h->H + CC - 1) / CC, nt, (int)(S * padded(h->Ny, fp64) * h->celem)};
 	h->sby1 = sub_batch(h->py, CC, maxe, &nt);
 	h->cy1 = {(h->H + CC - 1) / CC, nt, (int)(CC * padded(h->Ny, fp64) * h->celem)};
+	h->cxs = h->cx;
+	h->cys = h->cy;
+	if (rs && R == rs) h->cxs = {h->Ny / R, spec_x_threads(fp64, U, h->Nx), spec_x_smem(fp64, U, h->Nx), 1};
+	if (yspec) h->cys = {(h->H + CC - 1) / CC, spec_y_threads(fp64, U, h->Ny), spec_y_smem(fp64, U, h->Ny), 1};
+	return 0;
+}
+
+// Per-pass twiddle table of a compile-time length N (the layout of fft_core.cuh's
+// CtPlan): passes of radix rmain then one tail pass; pass p > 0 contributes
+// entries [(r - 1) * Ns + jm] = exp(-2 pi i r jm / (Ns R)).
+template <typename T> int upload_ct_twiddles(pfcg_handle* h, int N, int rmain, void** dst) {
+	int lg = 0;
+	while ((1 << lg) < N) lg++;
+	int lgm = 0;
+	while ((1 << lgm) < rmain) lgm++;
+	std::vector<int> radix;
+	for (int i = 0; i < lg / lgm; i++) radix.push_back(rmain);
+	if (lg % lgm) radix.push_back(1 << (lg % lgm));
+	std::vector<cplx<T>> tab;
+	int Ns = 1;
+	for (size_t p = 0; p < radix.size(); p++) {
+		const int R = radix[p];
+		if (p > 0)
+			for (int r = 1; r < R; r++)
+				for (int jm = 0; jm < Ns; jm++) {
+					const double a = -2.0 * PI * (double)r * (double)jm / ((double)Ns * R);
+					cplx<T> w;
+					w.x = (T)std::cos(a);
+					w.y = (T)std::sin(a);
+					tab.push_back(w);
+				}
+		Ns *= R;
+	}
+	if ((int)tab.size() != spec_twiddles(h->prec == PFCG_FP64, N)) return fail(h, PFCG_ESIZE, "twiddle table size mismatch");
+	CK(h, cudaMalloc(dst, sizeof(cplx<T>) * tab.size()));
+	CK(h, cudaMemcpy(*dst, tab.data(), sizeof(cplx<T>) * tab.size(), cudaMemcpyHostToDevice));
 	return 0;
 }
 
@@ -259,6 +315,7 @@ template <typename T> XArgs<T> xargs(pfcg_handle* h) {
 	a.acc = h->acc;
 	a.flag = h->flag;
 	a.tw = (const cplx<T>*)h->twx;
+	a.twct = (const cplx<T>*)h->twctx;
 	a.plan = h->px;
 	a.sb = h->sbx;
 	a.m = h->model;
@@ -275,6 +332,7 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.mean = h->mean;
 	a.acc = h->acc + ACC_NL;
 	a.tw = (const cplx<T>*)h->twy;
+	a.twct = (const cplx<T>*)h->twcty;
 	a.plan = h->py;
 	a.sb = h->sby;
 	a.m = h->model;
@@ -379,9 +437,9 @@ template <typename T> int do_steps(pfcg_handle* h, int nsteps) {
 	// evaluate (pfc-relax.c:1179-1185, 1125-1130); the y-pass does the same
 	// projection every step, so no separate pass is needed.
 	for (int s = 0; s < nsteps; s++) {
-		int rc = run_xpass<T>(h, XP_STEP, xa, h->cx);
+		int rc = run_xpass<T>(h, XP_STEP, xa, h->cxs);
 		if (rc) return rc;
-		rc = run_ypass<T>(h, YP_STEP, ya, h->cy);
+		rc = run_ypass<T>(h, YP_STEP, ya, h->cys);
 		if (rc) return rc;
 		h->t++;
 	}
@@ -535,6 +593,7 @@ template <typename T> int do_optimize(pfcg_handle* h, int xopt, int yopt, double
 	}
 	h->geom.dx = dx;
 	h->geom.dy = dy;
+	set_dk(h);
 	const double ddx = dx - dxs[0], ddy = dy - dys[0];
 	const double ddr = std::sqrt(ddx * ddx + ddy * ddy);
 	if (ddr < *d) *d *= 0.5;
@@ -585,6 +644,7 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	h->geom.H = h->H;
 	h->geom.dx = dx;
 	h->geom.dy = dy;
+	set_dk(h);
 	const bool fp64 = prec == PFCG_FP64;
 	h->celem = fp64 ? sizeof(double2) : sizeof(float2);
 	const int rmain = max_radix(fp64);
@@ -621,6 +681,10 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 #undef CKC
 	rc = fp64 ? upload_twiddles<double>(h, Nx, &h->twx) : upload_twiddles<float>(h, Nx, &h->twx);
 	if (!rc) rc = fp64 ? upload_twiddles<double>(h, Ny, &h->twy) : upload_twiddles<float>(h, Ny, &h->twy);
+	if (!rc && h->cxs.spec)
+		rc = fp64 ? upload_ct_twiddles<double>(h, Nx, rmain, &h->twctx) : upload_ct_twiddles<float>(h, Nx, rmain, &h->twctx);
+	if (!rc && h->cys.spec)
+		rc = fp64 ? upload_ct_twiddles<double>(h, Ny, rmain, &h->twcty) : upload_ct_twiddles<float>(h, Ny, rmain, &h->twcty);
 	if (rc) return bail(rc);
 	*out = h;
 	return 0;
@@ -634,6 +698,8 @@ void pfcg_destroy(pfcg_handle* h) {
 	cudaFree(h->work1);
 	cudaFree(h->twx);
 	cudaFree(h->twy);
+	cudaFree(h->twctx);
+	cudaFree(h->twcty);
 	cudaFree(h->mean);
 	cudaFree(h->acc);
 	cudaFree(h->offs);
@@ -662,6 +728,7 @@ int pfcg_set_box(pfcg_handle* h, double dx, double dy) {
 	if (!h) return PFCG_EARG;
 	h->geom.dx = dx;
 	h->geom.dy = dy;
+	set_dk(h);
 	return 0;
 }
 

@@ -304,4 +304,106 @@ __device__ __forceinline__ void fft_batches(cplx<T>* buf, int ld, int S, int SB,
 	}
 }
 
+// ------------------------------------------------- compile-time lengths --
+// Power-of-two lengths known at compile time: N = RM^A * RT. All index math
+// folds to shifts and masks; twiddles come from a per-pass table in shared
+// memory laid out [(r - 1) * Ns + jm] (consecutive threads read consecutive
+// words), entry = exp(-2 pi i r jm / (Ns R)).
+
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+
+template <int N, int RM> struct CtPlan {
+	static constexpr int LG = ilog2(N);
+	static constexpr int LGM = ilog2(RM);
+	static constexpr int A = LG / LGM;                 // passes of radix RM
+	static constexpr int RT = 1 << (LG % LGM);         // tail radix (1 = none)
+	static constexpr int NPASS = A + (RT > 1 ? 1 : 0);
+	__host__ __device__ static constexpr int radix(int p) { return p < A ? RM : RT; }
+	__host__ __device__ static constexpr int ns(int p) { return p == 0 ? 1 : ns(p - 1) * radix(p - 1); }
+	// twiddle-table offset of pass p (pass 0 has none)
+	__host__ __device__ static constexpr int twoff(int p) { return p <= 1 ? 0 : twoff(p - 1) + (radix(p - 1) - 1) * ns(p - 1); }
+	static constexpr int TWN = twoff(NPASS);
+};
+
+// pad(a + m * P) = pad(a) + m * (P + 1) for the padding period P = 2^SHIFT:
+// strides that are multiples of P become constant offsets from one padded base.
+template <int N, int R, int NS, int TWO, int NSEQ, int NT, int SIGN, typename T>
+__device__ __forceinline__ void ct_pass(cplx<T>* buf, const cplx<T>* tws, int t) {
+	constexpr int LD = N + (N >> Pad<T>::SHIFT) + 1;
+	constexpr int NR = N / R;
+	constexpr int TOTAL = NSEQ * NR;
+	constexpr int NB = (TOTAL + NT - 1) / NT;
+	constexpr int PP = 1 << Pad<T>::SHIFT;
+	cplx<T> v[NB][R];
+#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int b = t + i * NT;
+		if (TOTAL % NT == 0 || b < TOTAL) {
+			const int p = b / NR, j = b % NR;
+			const cplx<T>* in = buf + p * LD;
+			if constexpr (NR % PP == 0) {
+				const int pj = pad<T>(j);
+#pragma unroll
+				for (int r = 0; r < R; r++) v[i][r] = in[pj + r * (NR + NR / PP)];
+			} else {
+#pragma unroll
+				for (int r = 0; r < R; r++) v[i][r] = in[pad<T>(j + r * NR)];
+			}
+		}
+	}
+	__syncthreads();
+#pragma unroll
+	for (int i = 0; i < NB; i++) {
+		const int b = t + i * NT;
+		if (TOTAL % NT == 0 || b < TOTAL) {
+			const int p = b / NR, j = b % NR;
+			const int jm = j % NS;
+			if constexpr (NS > 1) {
+				const cplx<T>* twj = tws + TWO + jm;
+#pragma unroll
+				for (int r = 1; r < R; r++) {
+					cplx<T> w = twj[(r - 1) * NS];
+					if (SIGN > 0) w.y = -w.y;
+					v[i][r] = cmul(v[i][r], w);
+				}
+			}
+			dft<R, SIGN, T>(v[i]);
+			cplx<T>* out = buf + p * LD;
+			const int d0 = (j - jm) * R + jm;
+			if constexpr (NS % PP == 0) {
+				const int pd = pad<T>(d0);
+#pragma unroll
+				for (int r = 0; r < R; r++) out[pd + r * (NS + NS / PP)] = v[i][r];
+			} else if constexpr (NS == 1 && R <= PP && PP % R == 0) {
+				// d0 = j * R: the R outputs never cross a padding period
+				const int pd = pad<T>(d0);
+#pragma unroll
+				for (int r = 0; r < R; r++) out[pd + r] = v[i][r];
+			} else {
+#pragma unroll
+				for (int r = 0; r < R; r++) out[pad<T>(d0 + r * NS)] = v[i][r];
+			}
+		}
+	}
+	__syncthreads();
+}
+
+template <int N, int RM, int P, int NSEQ, int NT, int SIGN, typename T>
+__device__ __forceinline__ void ct_passes(cplx<T>* buf, const cplx<T>* tws, int t) {
+	using PL = CtPlan<N, RM>;
+	if constexpr (P < PL::NPASS) {
+		ct_pass<N, PL::radix(P), PL::ns(P), PL::twoff(P), NSEQ, NT, SIGN, T>(buf, tws, t);
+		ct_passes<N, RM, P + 1, NSEQ, NT, SIGN, T>(buf, tws, t);
+	}
+}
+
+// NSEQ resident sequences of compile-time length N (stride padded_len(N)),
+// transformed NSUB at a time by NT threads.
+template <int N, int RM, int NSEQ, int NSUB, int NT, int SIGN, typename T>
+__device__ __forceinline__ void fft_ct(cplx<T>* buf, const cplx<T>* tws, int t) {
+	constexpr int LD = N + (N >> Pad<T>::SHIFT) + 1;
+#pragma unroll 1
+	for (int b0 = 0; b0 < NSEQ; b0 += NSUB) ct_passes<N, RM, 0, NSUB, NT, SIGN, T>(buf + b0 * LD, tws, t);
+}
+
 } // namespace pfcg

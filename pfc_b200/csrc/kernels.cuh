@@ -49,6 +49,7 @@ struct Geom {
 	int R;      // rows per tile
 	int CC;     // columns per y-pass CTA
 	double dx, dy;
+	double dkx, dky;  // 2 pi / (dx Nx), 2 pi / (dy Ny), pfc-relax.c:916-917
 };
 
 enum XMode { XP_STEP = 0, XP_EVAL = 1, XP_C2R = 2, XP_R2C = 3 };
@@ -63,6 +64,7 @@ template <typename T> struct XArgs {
 	double* acc;            // FP64 accumulators (see kernels.cu)
 	int* flag;              // NaN flag
 	const cplx<T>* tw;      // twiddles of length Nx
+	const cplx<T>* twct;    // per-pass twiddle table of the specialised kernels
 	FftPlan plan;
 	int sb;                 // channel pairs per FFT call
 	Model m;
@@ -85,6 +87,7 @@ template <typename T> struct YArgs {
 	double* mean;           // U, updated in place by YP_STEP at k = 0
 	double* acc;            // FP64 sum of NL per field (read and cleared by YP_STEP)
 	const cplx<T>* tw;      // twiddles of length Ny
+	const cplx<T>* twct;    // per-pass twiddle table of the specialised kernels
 	FftPlan plan;
 	int sb;                 // sequences per FFT call
 	Model m;
@@ -95,7 +98,19 @@ template <typename T> struct YArgs {
 
 struct LaunchCfg {
 	int grid, block, smem;
+	int spec;  // 1: the compile-time specialised STEP kernel for this shape
 };
+
+// Shapes of the compile-time specialised STEP kernels (kernels_impl.cuh):
+// rows per x-pass tile and columns per y-pass CTA for length 2048 / 4096.
+int spec_rows(bool fp64, int U, int N);
+int spec_cols(bool fp64, int U, int N);
+// threads and shared-memory bytes of those kernels
+int spec_x_threads(bool fp64, int U, int N);
+int spec_y_threads(bool fp64, int U, int N);
+int spec_x_smem(bool fp64, int U, int N);
+int spec_y_smem(bool fp64, int U, int N);
+int spec_twiddles(bool fp64, int N);
 
 // Host-side launchers; return cudaGetLastError().
 template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s);

@@ -6,6 +6,41 @@ namespace pfcg {
 int max_elems_per_thread(bool fp64) { return fp64 ? FftCfg<double>::MAXE : FftCfg<float>::MAXE; }
 int max_radix(bool fp64) { return fp64 ? 8 : 16; }
 
+int spec_rows(bool fp64, int U, int N) {
+	if ((U != 1 && U != 2) || (N != 2048 && N != 4096)) return 0;
+	return fp64 ? Spec<double>::xr(U, N) : Spec<float>::xr(U, N);
+}
+int spec_cols(bool fp64, int U, int N) {
+	if ((U != 1 && U != 2) || (N != 2048 && N != 4096)) return 0;
+	return fp64 ? Spec<double>::ycc(U, N) : Spec<float>::ycc(U, N);
+}
+
+template <typename T> static int ct_twn(int N) { return N == 4096 ? CtPlan<4096, FftCfg<T>::MAXE>::TWN : CtPlan<2048, FftCfg<T>::MAXE>::TWN; }
+int spec_twiddles(bool fp64, int N) { return fp64 ? ct_twn<double>(N) : ct_twn<float>(N); }
+
+int spec_x_threads(bool fp64, int U, int N) {
+	const int maxe = max_elems_per_thread(fp64);
+	const int P = (U * spec_rows(fp64, U, N) + 1) / 2;
+	return P * N / maxe <= MAXNT ? P * N / maxe : MAXNT;
+}
+int spec_y_threads(bool fp64, int U, int N) {
+	const int maxe = max_elems_per_thread(fp64);
+	const int S = U * spec_cols(fp64, U, N);
+	return S * N / maxe <= MAXNT ? S * N / maxe : MAXNT;
+}
+int spec_x_smem(bool fp64, int U, int N) {
+	const int P = (U * spec_rows(fp64, U, N) + 1) / 2;
+	const int ce = fp64 ? 16 : 8;
+	const int ld = fp64 ? padded_len<double>(N) : padded_len<float>(N);
+	return (P * ld + spec_twiddles(fp64, N)) * ce;
+}
+int spec_y_smem(bool fp64, int U, int N) {
+	const int S = U * spec_cols(fp64, U, N);
+	const int ce = fp64 ? 16 : 8;
+	const int ld = fp64 ? padded_len<double>(N) : padded_len<float>(N);
+	return (S * ld + spec_twiddles(fp64, N)) * ce;
+}
+
 // ------------------------------------------------------ energy density --
 template <int U>
 __global__ void energy_density_kernel(const double* __restrict__ mf, const double* __restrict__ pn,

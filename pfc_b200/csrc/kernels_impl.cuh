@@ -58,11 +58,8 @@ template <typename T> __device__ __forceinline__ T expT(T x);
 template <> __device__ __forceinline__ float expT<float>(float x) { return expf(x); }
 template <> __device__ __forceinline__ double expT<double>(double x) { return exp(x); }
 
-// B = (exp(x) - 1)/a. FP64 follows pfc-relax.c:952 literally; FP32 uses expm1f,
-// which is the same quantity without the cancellation near a = 0.
-template <typename T> __device__ __forceinline__ T etd_b(T A, T x, T a);
-template <> __device__ __forceinline__ float etd_b<float>(float, float x, float a) { return expm1f(x) / a; }
-template <> __device__ __forceinline__ double etd_b<double>(double A, double, double a) { return (A - 1.0) / a; }
+// B = (exp(x) - 1)/a as pfc-relax.c:952 computes it (FP64 path; FP32 uses phi1f).
+template <typename T> __device__ __forceinline__ T etd_b(T A, T x, T a) { return (A - (T)1) / a; }
 
 // P_u(k^2) = prod_w (omega (nu2 - k2)^2 + phi), pfc-relax.c:943-947. Callers
 // pass a u that is a compile-time constant after unrolling, so nothing indexes
@@ -87,20 +84,71 @@ __device__ __forceinline__ double k2_of(int kx, int ky, const Geom& g, double dx
 	return kxv * kxv + kyv * kyv;
 }
 
+// k^2 of the current box with the wave-number steps precomputed on the host
+template <typename T> __device__ __forceinline__ T k2_step(int kx, int ky, int Ny, T dkx, T dky) {
+	const T kxv = (T)kx * dkx;
+	const T kyv = (T)(ky < Ny / 2 ? ky : ky - Ny) * dky;
+	return kxv * kxv + kyv * kyv;
+}
+
+// phi1(x) = (exp(x) - 1) / x given A = exp(x): Taylor series to x^6 / 7! for
+// |x| < 1/4 (remainder < 2e-9), the quotient otherwise (relative error below
+// 3e-7 in FP32). B = (A - 1)/a = o dt phi1(x) with x = o a dt, which is also
+// the reference's a = 0 case (pfc-relax.c:951-952).
+__device__ __forceinline__ float phi1f(float x, float A) {
+	if (fabsf(x) < 0.25f)
+		return 1.f + x * (0.5f + x * (1.f / 6.f + x * (1.f / 24.f + x * (1.f / 120.f + x * (1.f / 720.f + x * (1.f / 5040.f))))));
+	return (A - 1.f) / x;
+}
+
+// Launch shapes of the kernels specialised on a compile-time length NC (NC = 0:
+// runtime length and plan). P / S resident sequences, NSUB per FFT call, NT threads.
+template <typename T, int U, int NC, int RC> struct XCfg {
+	static constexpr bool CT = NC > 0;
+	static constexpr int MAXE = FftCfg<T>::MAXE;
+	static constexpr int P = CT ? (U * RC + 1) / 2 : 1;
+	static constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
+	static constexpr int NSUB = CT ? (P * NC / MAXE <= MAXNT ? P : MAXNT * MAXE / NC) : 1;
+	static constexpr int NT = CT ? NSUB * NC / MAXE : MAXNT;
+	static constexpr int MINB = (CT && sizeof(T) == 4) ? 2 : 1;
+	static constexpr int TWN = CT ? CtPlan<NC, MAXE>::TWN : 0;
+};
+
+template <typename T, int U, int NC, int CCC, int RC> struct YCfg {
+	static constexpr bool CT = NC > 0;
+	static constexpr int MAXE = FftCfg<T>::MAXE;
+	static constexpr int S = CT ? U * CCC : 1;
+	static constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
+	static constexpr int NSUB = CT ? (S * NC / MAXE <= MAXNT ? S : MAXNT * MAXE / NC) : 1;
+	static constexpr int NT = CT ? NSUB * NC / MAXE : MAXNT;
+	static constexpr int MINB = (CT && sizeof(T) == 4) ? 2 : 1;
+	static constexpr int TWN = CT ? CtPlan<NC, MAXE>::TWN : 0;
+};
+
 // ----------------------------------------------------------------- x-pass --
 
-template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 1) xpass_kernel(const XArgs<T> a) {
-	constexpr int MAXE = FftCfg<T>::MAXE;
+template <typename T, int U, int MODE, int NC, int RC>
+__global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MINB) xpass_kernel(const XArgs<T> a) {
+	using C = XCfg<T, U, NC, RC>;
+	constexpr int MAXE = C::MAXE;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
-	const int Nx = a.g.Nx, Ny = a.g.Ny, H = a.g.H, R = a.g.R;
+	const int Nx = C::CT ? NC : a.g.Nx;
+	const int Ny = a.g.Ny;
+	const int H = Nx / 2 + 1;
+	const int R = C::CT ? RC : a.g.R;
 	const int CH = U * R;
 	const int P = (CH + 1) >> 1;
-	const int ld = padded_len<T>(Nx);
+	const int ld = C::CT ? C::LD : padded_len<T>(Nx);
 	const int tile = blockIdx.x;
 	const int y0 = tile * R;
-	const int tid = threadIdx.x, nt = blockDim.x;
+	const int tid = threadIdx.x;
+	const int nt = C::CT ? C::NT : (int)blockDim.x;
 	const long long tofs = (long long)tile * H * R;
+	cplx<T>* tws = sm + (C::CT ? C::P * C::LD : 0);
+	if constexpr (C::CT) {
+		for (int i = tid; i < C::TWN; i += C::NT) tws[i] = a.twct[i];
+	}
 
 	double off[U];
 #pragma unroll
@@ -146,7 +194,8 @@ template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 
 			}
 		}
 		__syncthreads();
-		fft_batches<+1, MAXE, T>(sm, ld, P, a.sb, a.plan, a.tw, tid, nt);
+		if constexpr (C::CT) fft_ct<NC, MAXE, C::P, C::NSUB, C::NT, +1, T>(sm, tws, tid);
+		else fft_batches<+1, MAXE, T>(sm, ld, P, a.sb, a.plan, a.tw, tid, nt);
 	}
 
 	if constexpr (MODE == XP_STEP || MODE == XP_EVAL || MODE == XP_C2R) {
@@ -155,9 +204,10 @@ template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 
 #pragma unroll
 		for (int i = 0; i < NACC; i++) acc[i] = 0.0;
 		bool nan = false;
-		T lam[U], del[U], gam[U][U], alp[U][U];
+		T lam[U], del[U], gam[U][U], alp[U][U], offT[U];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
+			offT[u] = (T)off[u];
 			lam[u] = (T)a.m.lambda[u];
 			del[u] = (T)a.m.delta[u];
 #pragma unroll
@@ -180,7 +230,7 @@ template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 
 						T mv[U], mc[U];
 #pragma unroll
 						for (int u = 0; u < U; u++) {
-							mv[u] = z[r * U + u] + (T)off[u];
+							mv[u] = z[r * U + u] + offT[u];
 							nan |= (mv[u] != mv[u]);
 							mc[u] = (T)0;
 						}
@@ -239,7 +289,8 @@ template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 
 
 	if constexpr (MODE == XP_STEP || MODE == XP_R2C) {
 		__syncthreads();
-		fft_batches<-1, MAXE, T>(sm, ld, P, a.sb, a.plan, a.tw, tid, nt);
+		if constexpr (C::CT) fft_ct<NC, MAXE, C::P, C::NSUB, C::NT, -1, T>(sm, tws, tid);
+		else fft_batches<-1, MAXE, T>(sm, ld, P, a.sb, a.plan, a.tw, tid, nt);
 		// split each pair: Za = (C[k] + conj C[-k]) / 2, Zb = (C[k] - conj C[-k]) / (2i)
 		const T half = (T)0.5;
 		for (int k = tid; k < H; k += nt) {
@@ -266,6 +317,40 @@ template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 
 }
 
 // ----------------------------------------------------------------- y-pass --
+
+// Model constants of the k-space update converted once to the transform
+// precision (converting inside the per-entry loop costs an F2F per use).
+template <typename T, int U> struct StepConsts {
+	T invN, cc, dt, ag;
+	int W[U];
+	T alpha[U], betad[U];
+	T nu2[U][MAXW], omega[U][MAXW], phi[U][MAXW];
+	T beta[U][U], eps[U][U], mu2[U][U];
+	__device__ __forceinline__ StepConsts(const Model& m, int Nx, int Ny) {
+		invN = (T)(1.0 / ((double)Nx * (double)Ny));
+		cc = (T)m.c;
+		dt = (T)m.dt;
+		ag = (T)(-0.5 / m.sigma / m.sigma);
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			W[u] = m.W[u];
+			alpha[u] = (T)m.alpha[u][u];
+			betad[u] = (T)m.beta[u][u];
+#pragma unroll
+			for (int w = 0; w < MAXW; w++) {
+				nu2[u][w] = (T)m.nu2[u][w];
+				omega[u][w] = (T)m.omega[u][w];
+				phi[u][w] = (T)m.phi[u][w];
+			}
+#pragma unroll
+			for (int v = 0; v < U; v++) {
+				beta[u][v] = (T)m.beta[u][v];
+				eps[u][v] = (T)m.epsilon[u][v];
+				mu2[u][v] = (T)m.mu2[u][v];
+			}
+		}
+	}
+};
 
 // Hermitian projection of one resident column (kx = 0 or kx = Nx/2): entry ky
 // and entry Ny - ky become (a + conj b)/2 and its conjugate, self-conjugate
@@ -299,19 +384,30 @@ __device__ __forceinline__ void hermitian_column(cplx<T>* col, cplx<T>* spec_col
 	}
 }
 
-template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 1) ypass_kernel(const YArgs<T> a) {
-	constexpr int MAXE = FftCfg<T>::MAXE;
+template <typename T, int U, int MODE, int NC, int CCC, int RC>
+__global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC>::NT, YCfg<T, U, NC, CCC, RC>::MINB)
+    ypass_kernel(const YArgs<T> a) {
+	using C = YCfg<T, U, NC, CCC, RC>;
+	constexpr int MAXE = C::MAXE;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
-	const int Nx = a.g.Nx, Ny = a.g.Ny, H = a.g.H, R = a.g.R, CC = a.g.CC;
+	const int Nx = a.g.Nx, H = a.g.H;
+	const int Ny = C::CT ? NC : a.g.Ny;
+	const int R = C::CT ? RC : a.g.R;
+	const int CC = C::CT ? CCC : a.g.CC;
 	const int S = U * CC;
-	const int ld = padded_len<T>(Ny);
+	const int ld = C::CT ? C::LD : padded_len<T>(Ny);
 	const int kx0 = blockIdx.x * CC;
 	const int ncol = min(CC, H - kx0);
 	const int ntile = Ny / R;
 	const long long tileH = (long long)H * R;
 	const int chunk = CC * R;
-	const int tid = threadIdx.x, nt = blockDim.x;
+	const int tid = threadIdx.x;
+	const int nt = C::CT ? C::NT : (int)blockDim.x;
+	cplx<T>* tws = sm + (C::CT ? C::S * C::LD : 0);
+	if constexpr (C::CT) {
+		for (int i = tid; i < C::TWN; i += C::NT) tws[i] = a.twct[i];
+	}
 
 	if constexpr (MODE != YP_WEIGHT) {
 #pragma unroll
@@ -326,53 +422,86 @@ template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 
 			}
 		}
 		__syncthreads();
-		fft_batches<-1, MAXE, T>(sm, ld, S, a.sb, a.plan, a.tw, tid, nt);
+		if constexpr (C::CT) fft_ct<NC, MAXE, C::S, C::NSUB, C::NT, -1, T>(sm, tws, tid);
+		else fft_batches<-1, MAXE, T>(sm, ld, S, a.sb, a.plan, a.tw, tid, nt);
 	}
 
 	const double dx = a.g.dx, dy = a.g.dy;
 	if constexpr (MODE == YP_STEP) {
-		const T invN = (T)(1.0 / ((double)Nx * (double)Ny));
-		const T cc = (T)a.m.c;
-		const T dt = (T)a.m.dt;
-		const double ag = -0.5 / a.m.sigma / a.m.sigma;
-		for (int e = tid; e < CC * Ny; e += nt) {
-			const int c = e / Ny, ky = e - c * Ny;
-			if (c >= ncol) continue;
-			const int kx = kx0 + c;
-			const T k2 = (T)k2_of(kx, ky, a.g, dx, dy);
-			const long long si = (long long)kx * Ny + ky;
-			cplx<T> Nv[U], Mv[U];
+		// model constants in the transform precision, once per CTA
+		const StepConsts<T, U> K(a.m, Nx, Ny);
+		const T dkxT = (T)a.g.dkx, dkyT = (T)a.g.dky;
+		// update of one (kx, ky) entry for all fields, pfc-relax.c:1215-1244
+		auto update = [&](int c, int kx, int ky, const cplx<T>(&Nv)[U]) {
+			const T k2 = (sizeof(T) == 4) ? k2_step<T>(kx, ky, Ny, dkxT, dkyT) : (T)k2_of(kx, ky, a.g, dx, dy);
+			cplx<T> Mv[U];
 #pragma unroll
-			for (int u = 0; u < U; u++) {
-				Nv[u] = a.spec[u * a.sstride + si];
-				Mv[u] = cscale(sm[(u * CC + c) * ld + pad<T>(ky)], invN);
-			}
+			for (int u = 0; u < U; u++) Mv[u] = cscale(sm[(u * CC + c) * ld + pad<T>(ky)], K.invN);
 			if constexpr (U > 1) {
-				T G = expT<T>((T)ag * k2);
+				const T G = expT<T>(K.ag * k2);
 				const T G2 = G * G;
 #pragma unroll
 				for (int u = 0; u < U - 1; u++)
 #pragma unroll
 					for (int v = u + 1; v < U; v++) {
-						T d2 = (T)a.m.mu2[u][v] - k2;
+						T d2 = K.mu2[u][v] - k2;
 						d2 *= d2;
-						const T cu = (T)a.m.beta[u][v] * d2 + (T)a.m.epsilon[u][v] * G2;
+						const T cu = K.beta[u][v] * d2 + K.eps[u][v] * G2;
 						Mv[u] = cadd(Mv[u], cscale(Nv[v], cu));
 						Mv[v] = cadd(Mv[v], cscale(Nv[u], cu));
 					}
 			}
 			const bool origin = (kx == 0 && ky == 0);
+			const T o = K.cc - (T)1 - K.cc * k2;
 #pragma unroll
 			for (int u = 0; u < U; u++) {
-				const T av = (T)a.m.alpha[u][u] + (T)a.m.beta[u][u] * P_of<T>(a.m, u, k2);
-				const T o = cc - (T)1 - cc * k2;
-				const T x = o * av * dt;
+				T P = (T)1;
+#pragma unroll
+				for (int w = 0; w < MAXW; w++)
+					if (w < K.W[u]) {
+						const T q = K.nu2[u][w] - k2;
+						P *= K.omega[u][w] * q * q + K.phi[u][w];
+					}
+				const T av = K.alpha[u] + K.betad[u] * P;
+				const T x = o * av * K.dt;
 				const T A = expT<T>(x);
-				const T Bn = (av == (T)0) ? o * dt : etd_b<T>(A, x, av);
+				T Bn;
+				if constexpr (sizeof(T) == 4) Bn = o * K.dt * phi1f(x, A);
+				else Bn = (av == (T)0) ? o * K.dt : etd_b<T>(A, x, av);
 				cplx<T> nn = cadd(cscale(Nv[u], A), cscale(Mv[u], Bn));
 				if (origin) nn = mk<T>((T)0, (T)0);
-				a.spec[u * a.sstride + si] = nn;
+				a.spec[u * a.sstride + (long long)kx * Ny + ky] = nn;
 				sm[(u * CC + c) * ld + pad<T>(ky)] = nn;
+			}
+		};
+		if constexpr (C::CT && (CCC * NC) % C::NT == 0) {
+			// every thread owns PER entries: issue all spectral-state loads first
+			constexpr int PER = CCC * NC / C::NT;
+			cplx<T> Nv[PER][U];
+#pragma unroll
+			for (int i = 0; i < PER; i++) {
+				const int e = tid + i * C::NT;
+				const int c = e / NC, ky = e % NC;
+				const int kx = kx0 + c;
+#pragma unroll
+				for (int u = 0; u < U; u++)
+					Nv[i][u] = (c < ncol) ? a.spec[u * a.sstride + (long long)kx * NC + ky] : mk<T>((T)0, (T)0);
+			}
+#pragma unroll
+			for (int i = 0; i < PER; i++) {
+				const int e = tid + i * C::NT;
+				const int c = e / NC, ky = e % NC;
+				if (c < ncol) update(c, kx0 + c, ky, Nv[i]);
+			}
+		} else {
+			for (int e = tid; e < CC * Ny; e += nt) {
+				const int c = e / Ny, ky = e - c * Ny;
+				if (c >= ncol) continue;
+				const int kx = kx0 + c;
+				cplx<T> Nv[U];
+#pragma unroll
+				for (int u = 0; u < U; u++) Nv[u] = a.spec[u * a.sstride + (long long)kx * Ny + ky];
+				update(c, kx, ky, Nv);
 			}
 		}
 		if (kx0 == 0 && tid == 0) {
@@ -464,7 +593,8 @@ template <typename T, int U, int MODE> __global__ void __launch_bounds__(MAXNT, 
 		}
 	}
 	__syncthreads();
-	fft_batches<+1, MAXE, T>(sm, ld, S, a.sb, a.plan, a.tw, tid, nt);
+	if constexpr (C::CT) fft_ct<NC, MAXE, C::S, C::NSUB, C::NT, +1, T>(sm, tws, tid);
+	else fft_batches<+1, MAXE, T>(sm, ld, S, a.sb, a.plan, a.tw, tid, nt);
 
 #pragma unroll
 	for (int u = 0; u < U; u++) {
@@ -537,25 +667,56 @@ template <typename K> static void smem_attr(K k, unsigned long long& mask) {
 	cudaGetDevice(&dev);
 	const unsigned long long bit = 1ull << (dev & 63);
 	if (!(mask & bit)) {
-		cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+		int optin = 0;
+		cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+		cudaFuncAttributes fa;
+		cudaFuncGetAttributes(&fa, k);
+		cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 		mask |= bit;
 	}
 }
 
-template <typename T, int U, int MODE> static cudaError_t xlaunch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
-	auto k = xpass_kernel<T, U, MODE>;
+template <typename T, int U, int MODE, int NC, int RC>
+static cudaError_t xlaunch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	auto k = xpass_kernel<T, U, MODE, NC, RC>;
 	static unsigned long long mask = 0;
 	smem_attr(k, mask);
 	k<<<c.grid, c.block, c.smem, s>>>(a);
 	return cudaGetLastError();
 }
 
+// Compile-time specialisations of the STEP kernels: (length, rows per tile,
+// columns per y-pass CTA) for the sizes the workloads use; other sizes and
+// modes run the runtime-plan kernels.
+template <typename T> struct Spec;
+template <> struct Spec<float> {
+	// U = 1: x rows 4 (4096) / 8 (2048), y columns 2 / 4; U = 2: x rows 2 / 4, y columns 1 / 2
+	static constexpr int xr(int U, int N) { return U == 1 ? (N == 4096 ? 4 : 8) : (N == 4096 ? 2 : 4); }
+	static constexpr int ycc(int U, int N) { return U == 1 ? (N == 4096 ? 2 : 4) : (N == 4096 ? 1 : 2); }
+};
+template <> struct Spec<double> {
+	static constexpr int xr(int U, int N) { return U == 1 ? (N == 4096 ? 2 : 4) : (N == 4096 ? 1 : 2); }
+	static constexpr int ycc(int U, int N) { return U == 1 ? (N == 4096 ? 1 : 2) : 1; }
+};
+
+template <typename T, int U, int N> static bool x_is_spec(const XArgs<T>& a) {
+	return a.g.Nx == N && a.g.R == Spec<T>::xr(U, N);
+}
+template <typename T, int U, int N> static bool y_is_spec(const YArgs<T>& a) {
+	return a.g.Ny == N && a.g.CC == Spec<T>::ycc(U, N) && a.g.R == Spec<T>::xr(U, N);
+}
+
 template <typename T, int U> static cudaError_t xlaunch_mode(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
 	switch (mode) {
-	case XP_STEP: return xlaunch<T, U, XP_STEP>(a, c, s);
-	case XP_EVAL: return xlaunch<T, U, XP_EVAL>(a, c, s);
-	case XP_C2R: return xlaunch<T, U, XP_C2R>(a, c, s);
-	case XP_R2C: return xlaunch<T, U, XP_R2C>(a, c, s);
+	case XP_STEP:
+		if constexpr (U <= 2) {
+			if (c.spec && x_is_spec<T, U, 4096>(a)) return xlaunch<T, U, XP_STEP, 4096, Spec<T>::xr(U, 4096)>(a, c, s);
+			if (c.spec && x_is_spec<T, U, 2048>(a)) return xlaunch<T, U, XP_STEP, 2048, Spec<T>::xr(U, 2048)>(a, c, s);
+		}
+		return xlaunch<T, U, XP_STEP, 0, 0>(a, c, s);
+	case XP_EVAL: return xlaunch<T, U, XP_EVAL, 0, 0>(a, c, s);
+	case XP_C2R: return xlaunch<T, U, XP_C2R, 0, 0>(a, c, s);
+	case XP_R2C: return xlaunch<T, U, XP_R2C, 0, 0>(a, c, s);
 	}
 	return cudaErrorInvalidValue;
 }
@@ -570,35 +731,43 @@ template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, cons
 	return cudaErrorInvalidValue;
 }
 
-template <typename T, int U, int MODE> static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
-	auto k = ypass_kernel<T, U, MODE>;
+template <typename T, int U, int MODE, int NC, int CCC, int RC>
+static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	auto k = ypass_kernel<T, U, MODE, NC, CCC, RC>;
 	static unsigned long long mask = 0;
 	smem_attr(k, mask);
 	k<<<c.grid, c.block, c.smem, s>>>(a);
 	return cudaGetLastError();
 }
 
+template <typename T, int U> static cudaError_t ystep(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	if (c.spec && y_is_spec<T, U, 4096>(a))
+		return ylaunch<T, U, YP_STEP, 4096, Spec<T>::ycc(U, 4096), Spec<T>::xr(U, 4096)>(a, c, s);
+	if (c.spec && y_is_spec<T, U, 2048>(a))
+		return ylaunch<T, U, YP_STEP, 2048, Spec<T>::ycc(U, 2048), Spec<T>::xr(U, 2048)>(a, c, s);
+	return ylaunch<T, U, YP_STEP, 0, 0, 0>(a, c, s);
+}
+
 template <typename T> cudaError_t launch_ypass(int mode, const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
-	if (mode == YP_WEIGHT) return ylaunch<T, 1, YP_WEIGHT>(a, c, s);
+	if (mode == YP_WEIGHT) return ylaunch<T, 1, YP_WEIGHT, 0, 0, 0>(a, c, s);
 	if (mode == YP_STEP) {
 		switch (a.m.U) {
-		case 1: return ylaunch<T, 1, YP_STEP>(a, c, s);
-		case 2: return ylaunch<T, 2, YP_STEP>(a, c, s);
-		case 3: return ylaunch<T, 3, YP_STEP>(a, c, s);
-		case 4: return ylaunch<T, 4, YP_STEP>(a, c, s);
+		case 1: return ystep<T, 1>(a, c, s);
+		case 2: return ystep<T, 2>(a, c, s);
+		case 3: return ylaunch<T, 3, YP_STEP, 0, 0, 0>(a, c, s);
+		case 4: return ylaunch<T, 4, YP_STEP, 0, 0, 0>(a, c, s);
 		}
 	}
 	if (mode == YP_INIT) {
 		switch (a.m.U) {
-		case 1: return ylaunch<T, 1, YP_INIT>(a, c, s);
-		case 2: return ylaunch<T, 2, YP_INIT>(a, c, s);
-		case 3: return ylaunch<T, 3, YP_INIT>(a, c, s);
-		case 4: return ylaunch<T, 4, YP_INIT>(a, c, s);
+		case 1: return ylaunch<T, 1, YP_INIT, 0, 0, 0>(a, c, s);
+		case 2: return ylaunch<T, 2, YP_INIT, 0, 0, 0>(a, c, s);
+		case 3: return ylaunch<T, 3, YP_INIT, 0, 0, 0>(a, c, s);
+		case 4: return ylaunch<T, 4, YP_INIT, 0, 0, 0>(a, c, s);
 		}
 	}
 	return cudaErrorInvalidValue;
 }
-
 
 template <typename T>
 cudaError_t launch_kspace_energy(const cplx<T>* spec, long long sstride, const Model& m, const Geom& g, int ntrial,
