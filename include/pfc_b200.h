@@ -128,6 +128,32 @@ int pfcg_set_device(int device);
 int pfcg_set_profiling(pfcg_handle* h, int on);
 int pfcg_profile_read(pfcg_handle* h, double* ms, long long* launches, int nkinds);
 
+/* Bytes of the static device workspace of pfcg_relax_noalloc. */
+#define PFCG_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* One relaxation of nsteps steps without any device allocation. No counterpart
+ * in the reference: it exists for callers that cannot call cudaMalloc, such as
+ * a host application that hands out all device memory from its own pool and
+ * forbids other allocations, or a loop that must not pay cudaMalloc's implicit
+ * device synchronisation.
+ * fields: DEVICE memory, U*Ny*Nx doubles in the layout above; it holds the
+ *   initial fields on entry and the relaxed fields on return. The caller
+ *   allocates it; the call itself allocates nothing.
+ * stream: a cudaStream_t (NULL = the default stream); the call returns after it
+ *   has synchronised with that stream.
+ * Transforms run in FP32 (means and reductions in FP64), as PFCG_FP32.
+ * The workspace is a file-scope array of PFCG_NOALLOC_SCRATCH_BYTES (32 MiB)
+ * that every GPU loading the library holds until exit; grids needing more,
+ * about 2 * U * (Nx/2+1) * Ny * 8 bytes plus a few KB, are rejected with
+ * PFCG_ESIZE. The first call on a device takes the array's device address
+ * (cudaGetSymbolAddress) and sets kernel attributes; make that first call
+ * before any stream capture. All calls share the one array and it keeps the
+ * last call's contents (the call clears what must start at zero), so calls
+ * that overlap on the GPU (other streams, other host threads) race.
+ * Returns 0, 39 on NaN, or a negative PFCG_E* code (pfcg_last_error(NULL)). */
+int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double dx, double dy, int nsteps, double* fields,
+                       void* stream);
+
 /* The CUDA stream the handle launches on (a cudaStream_t), for timing. */
 int pfcg_stream(const pfcg_handle* h, void** stream);
 

@@ -806,3 +806,160 @@ int pfcg_launch_count(const pfcg_handle* h, long long* count) {
 const char* pfcg_last_error(const pfcg_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
 
 } // extern "C"
+
+// --------------------------------------------------------------- no-alloc ---
+// pfcg_relax_noalloc: a whole relaxation call (upload, steps, download) whose
+// device workspace lives in the file-scope array below instead of cudaMalloc'd
+// memory. Every GPU that loads this library holds the array until the process
+// exits. In host code g_noalloc_scratch names a host-side stand-in, not device
+// memory: its device address comes from cudaGetSymbolAddress, taken once per
+// device (with that device current) by the first call on it.
+
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PFCG_NOALLOC_SCRATCH_BYTES];
+
+void* g_noalloc_addr[64];
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// exp(-2 pi i k / n) in FP32 from a double-precision sincospi
+__global__ void noalloc_twiddles_kernel(float2* tw, int n) {
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		double sn, cs;
+		sincospi(-2.0 * (double)k / (double)n, &sn, &cs);
+		tw[k] = make_float2((float)cs, (float)sn);
+	}
+}
+
+// workspace bytes a call of this size needs (FP32 transforms)
+size_t noalloc_bytes(int U, int Nx, int Ny) {
+	const size_t nspec = (size_t)(Nx / 2 + 1) * Ny;
+	return 2 * align256(sizeof(float2) * nspec * U)       // spectral state, mixed workspace
+	       + align256(sizeof(double) * MAXU)               // means
+	       + align256(sizeof(double) * ACC_N)              // accumulators
+	       + align256(sizeof(int))                         // NaN flag
+	       + align256(sizeof(double) * MAXU * MEAN_BLOCKS) // partial sums of the means
+	       + align256(sizeof(float2) * Nx) + align256(sizeof(float2) * Ny);
+}
+
+} // namespace
+
+extern "C" int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double dx, double dy, int nsteps, double* fields,
+                                  void* stream) {
+	if (!p || !fields || nsteps < 0) return fail(nullptr, PFCG_EARG, "NULL argument or negative step count");
+	if (p->U < 1 || p->U > PFCG_MAX_U) return fail(nullptr, PFCG_EARG, "U out of range 1..4");
+	for (int u = 0; u < p->U; u++)
+		if (p->W[u] < 0 || p->W[u] > PFCG_MAX_W) return fail(nullptr, PFCG_EARG, "W[u] out of range 0..4");
+	if (!pfcg_size_supported(Nx, Ny))
+		return fail(nullptr, PFCG_ESIZE, "grid size not supported (need even 8..8192 with factors 2,3,5,7)");
+	const size_t need = noalloc_bytes(p->U, Nx, Ny);
+	if (need > (size_t)PFCG_NOALLOC_SCRATCH_BYTES)
+		return fail(nullptr, PFCG_ESIZE,
+		            "grid too large for pfcg_relax_noalloc: needs " + std::to_string(need) + " bytes of its " +
+		                std::to_string((size_t)PFCG_NOALLOC_SCRATCH_BYTES) + "-byte static workspace");
+	int dev = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e != cudaSuccess) return fail(nullptr, PFCG_ENODEV, cudaGetErrorString(e));
+	if (dev < 0 || dev >= 64) return fail(nullptr, PFCG_ENODEV, "device index out of range");
+	cudaDeviceProp prop;
+	e = cudaGetDeviceProperties(&prop, dev);
+	if (e != cudaSuccess) return fail(nullptr, PFCG_ENODEV, cudaGetErrorString(e));
+	if (prop.major != 10) return fail(nullptr, PFCG_ENODEV, "libpfc_b200 is built for sm_100a (B200) only");
+	if (!g_noalloc_addr[dev]) {
+		void* addr = nullptr;
+		e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+		if (e != cudaSuccess || !addr)
+			return fail(nullptr, PFCG_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+		g_noalloc_addr[dev] = addr;
+	}
+
+	// host-side description of the relaxation; no device memory is allocated
+	pfcg_handle h;
+	h.dev = dev;
+	h.prec = PFCG_FP32;
+	h.model = to_model(p);
+	h.U = p->U;
+	h.Nx = Nx;
+	h.Ny = Ny;
+	h.H = Nx / 2 + 1;
+	h.geom.Nx = Nx;
+	h.geom.Ny = Ny;
+	h.geom.H = h.H;
+	h.geom.dx = dx;
+	h.geom.dy = dy;
+	set_dk(&h);
+	h.celem = sizeof(float2);
+	h.stream = (cudaStream_t)stream;
+	int rc = 0;
+	if (!make_plan(Nx, max_radix(false), &h.px) || !make_plan(Ny, max_radix(false), &h.py))
+		rc = fail(&h, PFCG_ESIZE, "bad factorisation");
+	if (!rc) rc = choose_layout(&h, prop.multiProcessorCount);
+	if (rc) return fail(nullptr, rc, h.err);
+	// the runtime-plan STEP kernels (the specialised ones need per-pass tables)
+	h.cxs = h.cx;
+	h.cys = h.cy;
+
+	unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
+	const size_t nspec = (size_t)h.H * Ny;
+	size_t off = 0;
+	auto carve = [&](size_t bytes) {
+		void* q = base + off;
+		off += align256(bytes);
+		return q;
+	};
+	h.spec = carve(sizeof(float2) * nspec * h.U);
+	h.work = carve(sizeof(float2) * nspec * h.U);
+	h.mean = (double*)carve(sizeof(double) * MAXU);
+	h.acc = (double*)carve(sizeof(double) * ACC_N);
+	h.flag = (int*)carve(sizeof(int));
+	h.d_part = (double*)carve(sizeof(double) * MAXU * MEAN_BLOCKS);
+	h.twx = carve(sizeof(float2) * Nx);
+	h.twy = carve(sizeof(float2) * Ny);
+	h.d_real = fields; // the caller's buffer is both input and output
+
+	auto done = [&](int code) {
+		// the handle's pointers are views of the static workspace: nothing to free
+		h.spec = h.work = h.twx = h.twy = nullptr;
+		h.mean = h.acc = h.d_part = nullptr;
+		h.flag = nullptr;
+		h.d_real = nullptr;
+		return code ? fail(nullptr, code, h.err) : 0;
+	};
+#define CKN(call)                                                                                                      \
+	do {                                                                                                           \
+		cudaError_t e_ = (call);                                                                               \
+		if (e_ != cudaSuccess) return done(cuda_fail(&h, #call, e_));                                          \
+	} while (0)
+
+	// the workspace keeps the previous call's contents: clear what must start at zero
+	CKN(cudaMemsetAsync(h.acc, 0, sizeof(double) * ACC_N, h.stream));
+	CKN(cudaMemsetAsync(h.flag, 0, sizeof(int), h.stream));
+	noalloc_twiddles_kernel<<<(Nx + 255) / 256, 256, 0, h.stream>>>((float2*)h.twx, Nx);
+	CKN(cudaGetLastError());
+	noalloc_twiddles_kernel<<<(Ny + 255) / 256, 256, 0, h.stream>>>((float2*)h.twy, Ny);
+	CKN(cudaGetLastError());
+
+	// upload (means, r2c along x, FFT along y), steps, download
+	CKN(launch_field_means(fields, h.U, (long long)Nx * Ny, h.d_part, MEAN_BLOCKS, h.mean, h.stream));
+	XArgs<float> xa = xargs<float>(&h);
+	YArgs<float> ya = yargs<float>(&h);
+	if ((rc = run_xpass<float>(&h, XP_R2C, xa, h.cx))) return done(rc);
+	if ((rc = run_ypass<float>(&h, YP_INIT, ya, h.cy))) return done(rc);
+	xa.acc = h.acc + ACC_NL;
+	for (int s = 0; s < nsteps; s++) {
+		if ((rc = run_xpass<float>(&h, XP_STEP, xa, h.cxs))) return done(rc);
+		if ((rc = run_ypass<float>(&h, YP_STEP, ya, h.cys))) return done(rc);
+	}
+	xa.acc = h.acc;
+	if ((rc = run_xpass<float>(&h, XP_C2R, xa, h.cx))) return done(rc);
+	int nan = 0;
+	CKN(cudaMemcpyAsync(&nan, h.flag, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
+	CKN(cudaStreamSynchronize(h.stream));
+#undef CKN
+	if (nan) {
+		h.err = "Not a number value detected.";
+		return done(PFCG_NAN);
+	}
+	return done(0);
+}

@@ -23,6 +23,9 @@ OK = 0
 NAN = 39
 EARG, ECUDA, ESIZE, ENOMEM, ETIMEOUT, ENODEV = -1, -2, -3, -4, -5, -6
 
+# size of pfcg_relax_noalloc's static device workspace (PFCG_NOALLOC_SCRATCH_BYTES)
+NOALLOC_SCRATCH_BYTES = 32 << 20
+
 # every entry point of include/pfc_b200.h with its ctypes signature
 _vp, _ip, _dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
@@ -41,6 +44,8 @@ SIGNATURES = {
     "pfcg_set_device": (ctypes.c_int, [_ip]),
     "pfcg_set_profiling": (ctypes.c_int, [_vp, _ip]),
     "pfcg_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _ip]),
+    "pfcg_relax_noalloc": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_double, ctypes.c_double, _ip,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     "pfcg_stream": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
     "pfcg_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "pfcg_last_error": (ctypes.c_char_p, [_vp]),
@@ -221,3 +226,16 @@ class Relaxation:
             self.step(nxt - t)
             t = nxt
         return np.array(rows)
+
+
+def relax_noalloc(params: Params, Nx: int, Ny: int, dx: float, dy: float, nsteps: int, fields_dev_ptr: int,
+                  stream: int = 0) -> int:
+    """pfcg_relax_noalloc on a caller-owned DEVICE buffer (U*Ny*Nx doubles,
+    in/out). Returns the status code (0, 39 for NaN, negative on errors)."""
+    L = load()
+    return L.pfcg_relax_noalloc(ctypes.byref(params), Nx, Ny, dx, dy, nsteps, ctypes.c_void_p(fields_dev_ptr),
+                                ctypes.c_void_p(stream))
+
+
+def last_error() -> str:
+    return load().pfcg_last_error(None).decode()
