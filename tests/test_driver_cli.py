@@ -1,0 +1,166 @@
+"""The drop-in pfc-relax driver against the reference binary: the .in grammar,
+error messages and exit codes (CPU: the driver stops after parsing when
+PFC_B200_CHECK_ONLY=1), and whole runs on the GPU (marked gpu)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from pfc_b200 import lib, nfile, synth
+from pfc_b200 import params as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref", "pfc-relax")
+DRV = lib.DRIVER_PATH
+
+GOOD_1C = """# a comment line
+I\tin0.n
+\tout0-#.n\tf-#.f
+\t10\t[\t0\t20\t]\t12\t6
+M\t1
+l\t0.0
+a\t-0.25
+b\t1.0
+g\t0.0
+d\t1.0
+e\t
+s\t0.2
+n\t1.0
+o\t1.0
+p\t0.0
+m\t
+R\t1\t20\t0.785\t0.785\t1.0\t0\t1\t1
+"""
+
+
+def run(binary, cwd, args=("x.in",), env_extra=None):
+    env = dict(os.environ)
+    env["PFC_B200_CHECK_ONLY"] = "1"
+    if env_extra:
+        env.update(env_extra)
+    r = subprocess.run([binary] + list(args), cwd=cwd, capture_output=True, text=True, env=env, timeout=120)
+    return r.returncode, r.stdout
+
+
+def setup_case(tmp_path, text, data=True, Nx=16, Ny=16, header=None, values=None):
+    (tmp_path / "x.in").write_text(text)
+    if data:
+        f = synth.noise_state(Nx, Ny, 0.25, 0.05, 1)
+        body = header if header is not None else "%d %d 0.785 0.785\n" % (Nx, Ny)
+        vals = values if values is not None else "".join("%.12e\n" % v for v in f.ravel())
+        (tmp_path / "in0.n").write_text(body + vals)
+
+
+def mutate(old, new):
+    assert old in GOOD_1C
+    return GOOD_1C.replace(old, new)
+
+
+CASES = [
+    ("missing_input", None, 0),
+    ("multichar", "XY\n" + GOOD_1C, 1),
+    ("missing_data_file", mutate("I\tin0.n", "I\tnope.n"), 3),
+    ("bad_outputs", mutate("\tout0-#.n\tf-#.f", "\ta\tb\tc"), 6),
+    ("bad_write_params", mutate("\t10\t[\t0\t20\t]\t12\t6", "\t10\t20\t12\t6\t7"), 9),
+    ("write_steps_not_increasing", mutate("[\t0\t20\t]", "[\t20\t0\t]"), 10),
+    ("write_no_bracket", mutate("[\t0\t20\t]", "(\t0\t20\t]"), 9),
+    ("field_count", mutate("M\t1", "M\t2"), 12),
+    ("no_omega_label", mutate("o\t1.0\n", ""), 29),
+    ("bad_lambda", mutate("l\t0.0", "l\tzero"), 14),
+    ("bad_relax_line", mutate("R\t1\t20\t0.785\t0.785\t1.0\t0\t1\t1", "R\t1\t20\t0.785"), 35),
+    ("unknown_label", GOOD_1C + "Z\n", 36),
+]
+
+
+@pytest.mark.parametrize("name,text,code", CASES)
+def test_error_codes_match_reference(tmp_path, name, text, code):
+    if text is not None:
+        setup_case(tmp_path, text)
+    got = run(DRV, tmp_path)
+    ref = run(REF, tmp_path)
+    assert ref[0] == code, (name, ref)
+    assert got == ref, (name, got, ref)
+
+
+@pytest.mark.parametrize("name,header,values,code", [
+    ("bad_header", "16 x 0.785 0.785\n", None, 4),
+    ("three_number_header", "16 16 0.785\n", None, 38),
+    ("bad_value", None, "0.1\n" * 100 + "abc\n", 38),
+    ("short_file", None, "0.1\n" * 100, 38),
+])
+def test_data_file_errors_match_reference(tmp_path, name, header, values, code):
+    setup_case(tmp_path, GOOD_1C, header=header, values=values)
+    got = run(DRV, tmp_path)
+    ref = run(REF, tmp_path)
+    assert ref[0] == code, (name, ref)
+    assert got == ref, (name, got, ref)
+
+
+def test_mismatched_dimensions(tmp_path):
+    text = mutate("I\tin0.n", "I\tin0.n\tin1.n").replace("\tout0-#.n\tf-#.f", "\tout0-#.n\tout1-#.n")
+    setup_case(tmp_path, text)
+    (tmp_path / "in1.n").write_text("8 8 0.7 0.7\n" + "0.1\n" * 64)
+    got = run(DRV, tmp_path)
+    ref = run(REF, tmp_path)
+    assert ref[0] == 5 and got == ref
+
+
+def test_bad_argument_count(tmp_path):
+    got = run(DRV, tmp_path, args=("a.in", "b.in"))
+    ref = run(REF, tmp_path, args=("a.in", "b.in"))
+    assert ref[0] == 41 and got == ref
+
+
+def test_valid_input_parses(tmp_path):
+    setup_case(tmp_path, GOOD_1C)
+    code, out = run(DRV, tmp_path)
+    assert code == 0 and out.startswith("ok U=1 Nx=16 Ny=16 tend=20 Tprint=10 nwrite=2")
+
+
+def full_case(d, precision_env=None):
+    pd = P.hetero_2c(0.04)
+    Nx = Ny = 48
+    dx = dy = 0.7
+    f = synth.stripes2(Nx, Ny, dx, dy, 12, (0.3, -0.3), (0.3, 0.3), (7.2552, 7.2552 * 1.04), 0.02, 5)
+    for u in range(2):
+        nfile.write_n(os.path.join(d, "in%d.n" % u), f[u], dx, dy, 17)
+    nfile.write_input(os.path.join(d, "case.in"), ["in0.n", "in1.n"], ["a-#.n0", "a-#.n1"], "a-#.f", Tprint=25,
+                      twrite=[0, 30, 100, 150], pprint=12, pwrite=12, params=pd, c=1.0, tend=150, dx=dx, dy=dy,
+                      dt=0.25, Topt=50, xopt=1, yopt=1)
+
+
+@pytest.mark.gpu
+def test_full_run_matches_reference(tmp_path):
+    """Both binaries on the same input: the .out rows (t, dx, dy, <f>, <n_u>;
+    the wall-seconds column aside), the names, headers and values of every
+    written .n and .f file. The .f at t = 30 is the f(r) of the last evaluate
+    (t = 25), as the reference writes it."""
+    dirs = {}
+    for name, exe in (("ref", REF), ("gpu", DRV)):
+        d = tmp_path / name
+        d.mkdir()
+        full_case(str(d))
+        env = dict(os.environ)
+        env.pop("PFC_B200_CHECK_ONLY", None)
+        r = subprocess.run([exe, "case.in"], cwd=d, capture_output=True, text=True, env=env, timeout=600)
+        assert r.returncode == 0, (name, r.stdout, r.stderr)
+        dirs[name] = d
+    ro = nfile.read_out(str(dirs["ref"] / "case.out"))
+    go = nfile.read_out(str(dirs["gpu"] / "case.out"))
+    assert ro.shape == go.shape
+    np.testing.assert_allclose(go[:, 0], ro[:, 0])
+    np.testing.assert_allclose(go[:, 2:], ro[:, 2:], rtol=1e-9, atol=1e-12)
+    names = sorted(p.name for p in dirs["ref"].iterdir() if p.suffix in (".n0", ".n1", ".f"))
+    assert names == sorted(p.name for p in dirs["gpu"].iterdir() if p.suffix in (".n0", ".n1", ".f"))
+    assert len(names) == 12
+    for n in names:
+        rt = (dirs["ref"] / n).read_text().splitlines()
+        gt = (dirs["gpu"] / n).read_text().splitlines()
+        assert len(rt) == len(gt) == 48 * 48 + 1
+        rh, gh = rt[0].split(), gt[0].split()
+        assert rh[:2] == gh[:2]
+        np.testing.assert_allclose([float(x) for x in gh[2:]], [float(x) for x in rh[2:]], rtol=1e-9)
+        np.testing.assert_allclose(np.array(gt[1:], float), np.array(rt[1:], float), rtol=0, atol=1e-8, err_msg=n)
+        # number formatting: "%.12e" lines
+        assert all(len(line.split("e")[0].split(".")[1]) == 12 for line in gt[1:50])
