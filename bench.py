@@ -190,6 +190,7 @@ def main():
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT reference timing")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -301,6 +302,24 @@ def main():
            "d2h_bytes_per_step": int((hout.nbytes + 8 * (1 + U)) / args.steps),
            "note": "one relaxation call sequence per run: upload, %d steps, evaluate, download" % args.steps}
 
+    # cuFFT beside the step, as a reference point only: the FFT work of one step
+    # (forward r2c and inverse c2r of all U fields) through torch.fft
+    cufft = None
+    if rank == 0 and not args.no_cufft:
+        x = torch.randn((U, N, N), device="cuda", dtype=torch.float32 if main_p == "fp32" else torch.float64)
+        for _ in range(3):
+            y = torch.fft.irfft2(torch.fft.rfft2(x), s=(N, N))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(20):
+            y = torch.fft.irfft2(torch.fft.rfft2(x), s=(N, N))
+        e1.record()
+        torch.cuda.synchronize()
+        cufft = {"ms_r2c_plus_c2r": e0.elapsed_time(e1) / 20, "what": "torch.fft rfft2 + irfft2 of the U fields (cuFFT)"}
+        del x, y
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(N, U, rank, args.cpu_steps)
@@ -329,6 +348,8 @@ def main():
                         "fave": r64["fave"], "rel_dF_vs_fp32": abs(res["fave"] - r64["fave"]) / abs(r64["fave"])}
     if cpu:
         line["cpu_baseline"] = cpu
+    if cufft:
+        line["cufft_reference"] = cufft
     if rank == 0:
         print(json.dumps(line))
     for v in results.values():

@@ -312,13 +312,17 @@ __device__ __forceinline__ void fft_batches(cplx<T>* buf, int ld, int S, int SB,
 
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
 
+// The tail radix, when there is one, is pass 1 (second), so that the first and
+// the last pass both have radix RM: the last pass then leaves in each thread
+// exactly the elements the next transform's first pass needs (fused below).
 template <int N, int RM> struct CtPlan {
 	static constexpr int LG = ilog2(N);
 	static constexpr int LGM = ilog2(RM);
 	static constexpr int A = LG / LGM;                 // passes of radix RM
 	static constexpr int RT = 1 << (LG % LGM);         // tail radix (1 = none)
 	static constexpr int NPASS = A + (RT > 1 ? 1 : 0);
-	__host__ __device__ static constexpr int radix(int p) { return p < A ? RM : RT; }
+	static constexpr bool FUSABLE = A >= 2;            // first and last pass both radix RM
+	__host__ __device__ static constexpr int radix(int p) { return (RT > 1 && p == 1) ? RT : RM; }
 	__host__ __device__ static constexpr int ns(int p) { return p == 0 ? 1 : ns(p - 1) * radix(p - 1); }
 	// twiddle-table offset of pass p (pass 0 has none)
 	__host__ __device__ static constexpr int twoff(int p) { return p <= 1 ? 0 : twoff(p - 1) + (radix(p - 1) - 1) * ns(p - 1); }
@@ -395,6 +399,122 @@ __device__ __forceinline__ void ct_passes(cplx<T>* buf, const cplx<T>* tws, int 
 		ct_pass<N, PL::radix(P), PL::ns(P), PL::twoff(P), NSEQ, NT, SIGN, T>(buf, tws, t);
 		ct_passes<N, RM, P + 1, NSEQ, NT, SIGN, T>(buf, tws, t);
 	}
+}
+
+template <int N, int RM, int P, int NSEQ, int NT, int SIGN, typename T>
+__device__ __forceinline__ void ct_middle_from(cplx<T>* buf, const cplx<T>* tws, int t) {
+	using PL = CtPlan<N, RM>;
+	if constexpr (P < PL::NPASS - 1) {
+		ct_pass<N, PL::radix(P), PL::ns(P), PL::twoff(P), NSEQ, NT, SIGN, T>(buf, tws, t);
+		ct_middle_from<N, RM, P + 1, NSEQ, NT, SIGN, T>(buf, tws, t);
+	}
+}
+
+// ------------------------------------------------------ fused first/last --
+// In a pass of radix RM, butterfly b = t + i*NT of the NSEQ sequences handles
+// sequence p = b / (N/RM) at positions j + r*N/RM (j = b mod N/RM): the first
+// pass (Ns = 1) reads them and the last pass (Ns = N/RM) writes them. RegBlock
+// holds one thread's elements between the two, so pointwise work and global
+// loads/stores can act on them in registers.
+// Thread-to-butterfly maps of a fused pass: StdMap is b = t + i*NT;
+// PairMap (two fields of CC columns, one butterfly per thread) puts field 0
+// in lanes 0-15 and field 1 in lanes 16-31 of each warp at the same butterfly,
+// so lane l and lane l ^ 16 hold the two fields at the same points.
+template <int N, int RM, int NSEQ, int NT> struct StdMap {
+	static constexpr int NR = N / RM;
+	static constexpr int NB = (NSEQ * NR + NT - 1) / NT;
+	static_assert((NSEQ * NR) % NT == 0, "whole butterflies per thread");
+	__device__ __forceinline__ static int seq(int t, int i) { return (t + i * NT) / NR; }
+	__device__ __forceinline__ static int bj(int t, int i) { return (t + i * NT) % NR; }
+};
+
+template <int N, int RM, int CC> struct PairMap {
+	static constexpr int NR = N / RM;
+	static constexpr int NB = 1;
+	__device__ __forceinline__ static int field(int t) { return (t >> 4) & 1; }
+	__device__ __forceinline__ static int rest(int t) { return ((t >> 5) << 4) | (t & 15); }
+	__device__ __forceinline__ static int col(int t) { return rest(t) / NR; }
+	__device__ __forceinline__ static int seq(int t, int) { return field(t) * CC + col(t); }
+	__device__ __forceinline__ static int bj(int t, int) { return rest(t) % NR; }
+};
+
+template <int N, int RM, int NSEQ, int NT, typename T, typename MAP = StdMap<N, RM, NSEQ, NT>> struct RegBlock {
+	static constexpr int NR = N / RM;
+	static constexpr int NB = MAP::NB;
+	cplx<T> v[NB][RM];
+	__device__ __forceinline__ static int seq(int t, int i) { return MAP::seq(t, i); }
+	__device__ __forceinline__ static int pos(int t, int i, int r) { return MAP::bj(t, i) + r * NR; }
+};
+
+// first pass of a transform (Ns = 1) from registers to shared memory
+template <int N, int RM, int NSEQ, int NT, int SIGN, typename T, typename MAP = StdMap<N, RM, NSEQ, NT>>
+__device__ __forceinline__ void ct_first_from_regs(cplx<T>* buf, RegBlock<N, RM, NSEQ, NT, T, MAP>& rb, int t) {
+	constexpr int LD = N + (N >> Pad<T>::SHIFT) + 1;
+	constexpr int PP = 1 << Pad<T>::SHIFT;
+#pragma unroll
+	for (int i = 0; i < MAP::NB; i++) dft<RM, SIGN, T>(rb.v[i]);
+	__syncthreads(); // earlier readers of buf are done
+#pragma unroll
+	for (int i = 0; i < MAP::NB; i++) {
+		const int p = MAP::seq(t, i), j = MAP::bj(t, i);
+		cplx<T>* out = buf + p * LD;
+		const int d0 = j * RM;
+		if constexpr (RM <= PP && PP % RM == 0) {
+			const int pd = pad<T>(d0);
+#pragma unroll
+			for (int r = 0; r < RM; r++) out[pd + r] = rb.v[i][r];
+		} else {
+#pragma unroll
+			for (int r = 0; r < RM; r++) out[pad<T>(d0 + r)] = rb.v[i][r];
+		}
+	}
+	__syncthreads();
+}
+
+// last pass of a transform (Ns = N/RM) from shared memory into registers
+template <int N, int RM, int NSEQ, int NT, int SIGN, typename T, typename MAP = StdMap<N, RM, NSEQ, NT>>
+__device__ __forceinline__ void ct_last_to_regs(const cplx<T>* buf, const cplx<T>* tws,
+                                               RegBlock<N, RM, NSEQ, NT, T, MAP>& rb, int t) {
+	using PL = CtPlan<N, RM>;
+	constexpr int LD = N + (N >> Pad<T>::SHIFT) + 1;
+	constexpr int NR = N / RM;
+	constexpr int NS = NR;
+	constexpr int TWO = PL::twoff(PL::NPASS - 1);
+	constexpr int PP = 1 << Pad<T>::SHIFT;
+	static_assert(PL::ns(PL::NPASS - 1) == NS, "last pass of radix RM");
+#pragma unroll
+	for (int i = 0; i < MAP::NB; i++) {
+		const int p = MAP::seq(t, i), j = MAP::bj(t, i);
+		const cplx<T>* in = buf + p * LD;
+		if constexpr (NR % PP == 0) {
+			const int pj = pad<T>(j);
+#pragma unroll
+			for (int r = 0; r < RM; r++) rb.v[i][r] = in[pj + r * (NR + NR / PP)];
+		} else {
+#pragma unroll
+			for (int r = 0; r < RM; r++) rb.v[i][r] = in[pad<T>(j + r * NR)];
+		}
+	}
+	// no barrier needed here: the caller works on registers and the next write
+	// to this buffer is preceded by one
+#pragma unroll
+	for (int i = 0; i < MAP::NB; i++) {
+		const int j = MAP::bj(t, i); // jm = j since Ns = N/RM
+		const cplx<T>* twj = tws + TWO + j;
+#pragma unroll
+		for (int r = 1; r < RM; r++) {
+			cplx<T> w = twj[(r - 1) * NS];
+			if (SIGN > 0) w.y = -w.y;
+			rb.v[i][r] = cmul(rb.v[i][r], w);
+		}
+		dft<RM, SIGN, T>(rb.v[i]);
+	}
+}
+
+// the passes strictly between the first and the last, shared memory to shared memory
+template <int N, int RM, int NSEQ, int NT, int SIGN, typename T>
+__device__ __forceinline__ void ct_middle(cplx<T>* buf, const cplx<T>* tws, int t) {
+	ct_middle_from<N, RM, 1, NSEQ, NT, SIGN, T>(buf, tws, t);
 }
 
 // NSEQ resident sequences of compile-time length N (stride padded_len(N)),

@@ -98,7 +98,7 @@ template <typename T> struct YArgs {
 
 struct LaunchCfg {
 	int grid, block, smem;
-	int spec;  // 1: the compile-time specialised STEP kernel for this shape
+	int spec;  // 1: the compile-time specialised STEP kernel for this shape (2: never the fused y-pass)
 };
 
 // Shapes of the compile-time specialised STEP kernels (kernels_impl.cuh):
@@ -107,7 +107,7 @@ int spec_rows(bool fp64, int U, int N);
 int spec_cols(bool fp64, int U, int N);
 // threads and shared-memory bytes of those kernels
 int spec_x_threads(bool fp64, int U, int N);
-int spec_y_threads(bool fp64, int U, int N);
+int spec_y_threads(bool fp64, int U, int N, bool fused);
 int spec_x_smem(bool fp64, int U, int N);
 int spec_y_smem(bool fp64, int U, int N);
 int spec_twiddles(bool fp64, int N);

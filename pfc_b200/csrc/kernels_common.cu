@@ -23,10 +23,14 @@ int spec_x_threads(bool fp64, int U, int N) {
 	const int P = (U * spec_rows(fp64, U, N) + 1) / 2;
 	return P * N / maxe <= MAXNT ? P * N / maxe : MAXNT;
 }
-int spec_y_threads(bool fp64, int U, int N) {
+int spec_y_threads(bool fp64, int U, int N, bool fused) {
+	// fused y-pass: one thread per (field, column, butterfly); otherwise as many
+	// sequences per FFT call as fit MAXNT threads
 	const int maxe = max_elems_per_thread(fp64);
 	const int S = U * spec_cols(fp64, U, N);
-	return S * N / maxe <= MAXNT ? S * N / maxe : MAXNT;
+	if (fused && U <= 2 && S * N / maxe <= MAXNT) return S * N / maxe;
+	if (S * N / maxe <= MAXNT) return S * N / maxe;
+	return MAXNT;
 }
 int spec_x_smem(bool fp64, int U, int N) {
 	const int P = (U * spec_rows(fp64, U, N) + 1) / 2;

@@ -16,6 +16,8 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace pfcg {
@@ -114,16 +116,357 @@ template <typename T, int U, int NC, int RC> struct XCfg {
 	static constexpr int TWN = CT ? CtPlan<NC, MAXE>::TWN : 0;
 };
 
-template <typename T, int U, int NC, int CCC, int RC> struct YCfg {
+template <typename T, int U, int NC, int CCC, int RC, bool FUSEDK = true> struct YCfg {
 	static constexpr bool CT = NC > 0;
 	static constexpr int MAXE = FftCfg<T>::MAXE;
 	static constexpr int S = CT ? U * CCC : 1;
 	static constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
-	static constexpr int NSUB = CT ? (S * NC / MAXE <= MAXNT ? S : MAXNT * MAXE / NC) : 1;
-	static constexpr int NT = CT ? NSUB * NC / MAXE : MAXNT;
+	static constexpr bool FUSED = FUSEDK && CT && CtPlan<(CT ? NC : 256), MAXE>::FUSABLE && U <= 2 &&
+	                              U * CCC * (CT ? NC : 256) / MAXE <= MAXNT;
+	static constexpr int NSUB = CT ? (FUSED ? S : (S * NC / MAXE <= MAXNT ? S : MAXNT * MAXE / NC)) : 1;
+	// fused: thread t holds butterfly t mod N/MAXE of column t / (N/MAXE) for every field
+	static constexpr int NT = CT ? (FUSED ? U * CCC * NC / MAXE : NSUB * NC / MAXE) : MAXNT;
 	static constexpr int MINB = (CT && sizeof(T) == 4) ? 2 : 1;
 	static constexpr int TWN = CT ? CtPlan<NC, MAXE>::TWN : 0;
 };
+
+// Model constants of the k-space update converted once to the transform
+// precision (converting inside the per-entry loop costs an F2F per use).
+template <typename T, int U> struct StepConsts {
+	T invN, cc, dt, ag;
+	int W[U];
+	T alpha[U], betad[U];
+	T nu2[U][MAXW], omega[U][MAXW], phi[U][MAXW];
+	T beta[U][U], eps[U][U], mu2[U][U];
+	__device__ __forceinline__ StepConsts(const Model& m, int Nx, int Ny) {
+		invN = (T)(1.0 / ((double)Nx * (double)Ny));
+		cc = (T)m.c;
+		dt = (T)m.dt;
+		ag = (T)(-0.5 / m.sigma / m.sigma);
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			W[u] = m.W[u];
+			alpha[u] = (T)m.alpha[u][u];
+			betad[u] = (T)m.beta[u][u];
+#pragma unroll
+			for (int w = 0; w < MAXW; w++) {
+				nu2[u][w] = (T)m.nu2[u][w];
+				omega[u][w] = (T)m.omega[u][w];
+				phi[u][w] = (T)m.phi[u][w];
+			}
+#pragma unroll
+			for (int v = 0; v < U; v++) {
+				beta[u][v] = (T)m.beta[u][v];
+				eps[u][v] = (T)m.epsilon[u][v];
+				mu2[u][v] = (T)m.mu2[u][v];
+			}
+		}
+	}
+};
+
+// Hermitian projection of one resident column (kx = 0 or kx = Nx/2): entry ky
+// and entry Ny - ky become (a + conj b)/2 and its conjugate, self-conjugate
+// entries become real. Writes shared memory and the spectral state. This is
+// the reference's resynchronisation N^ = FFT(c2r(N^)) (pfc-relax.c:1179-1185)
+// restricted to the only columns where it is not the identity, done every
+// step: their anti-Hermitian part is invisible to c2r and is not acted on by
+// the nonlinear term, so between resyncs it grows like A(k)^t for every
+// unstable k (x1.28 per step for epsilon = -0.25, dt = 1), which overflows in FP32.
+template <typename T>
+__device__ __forceinline__ void hermitian_column(cplx<T>* col, cplx<T>* spec_col, int Ny, int tid, int nt) {
+	const int half = Ny / 2;
+	for (int base = 0; base <= half; base += nt) {
+		const int j = base + tid;
+		cplx<T> p = mk<T>((T)0, (T)0);
+		const int jn = (Ny - j) % Ny;
+		if (j <= half) {
+			const cplx<T> a = col[pad<T>(j)], b = col[pad<T>(jn)];
+			p = mk<T>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y));
+		}
+		__syncthreads();
+		if (j <= half) {
+			col[pad<T>(j)] = p;
+			spec_col[j] = p;
+			if (jn != j) {
+				col[pad<T>(jn)] = cconj(p);
+				spec_col[jn] = cconj(p);
+			}
+		}
+		__syncthreads();
+	}
+}
+
+// ------------------------------------------------ fused step pipelines --
+// Specialised lengths whose first and last FFT pass have the same radix keep
+// each thread's elements in registers from the last pass of one transform to
+// the first pass of the next (fft_core.cuh, RegBlock), so the pointwise work
+// between two transforms costs no shared-memory round trip and no barrier.
+
+template <typename T, int U> __device__ __forceinline__ T pick(const T (&a)[U], int u) {
+	T r = a[0];
+#pragma unroll
+	for (int k = 1; k < U; k++)
+		if (u == k) r = a[k];
+	return r;
+}
+
+// k = 0 in FP64 (one thread): mean' = A(0) mean + B(0) (sum NL + couplings),
+// pfc-relax.c:1215-1244 at k = 0; clears the NL sums for the next step
+template <typename T, int U> __device__ __forceinline__ void ypass_mean_update(const YArgs<T>& a) {
+	const double NxNy = (double)a.g.Nx * (double)a.g.Ny;
+	double mean0[U], Mk[U];
+#pragma unroll
+	for (int u = 0; u < U; u++) { mean0[u] = a.mean[u]; Mk[u] = a.acc[u]; }
+#pragma unroll
+	for (int u = 0; u < U - 1; u++)
+#pragma unroll
+		for (int v = u + 1; v < U; v++) {
+			const double d2 = a.m.mu2[u][v] * a.m.mu2[u][v];
+			const double cu = a.m.beta[u][v] * d2 + a.m.epsilon[u][v];
+			Mk[u] += cu * mean0[v] * NxNy;
+			Mk[v] += cu * mean0[u] * NxNy;
+		}
+#pragma unroll
+	for (int u = 0; u < U; u++) {
+		const double P0 = P_of<double>(a.m, u, 0.0);
+		const double av = a.m.alpha[u][u] + a.m.beta[u][u] * P0;
+		const double o = a.m.c - 1.0;
+		const double A = exp(o * av * a.m.dt);
+		const double B = ((av == 0.0) ? o * a.m.dt : (A - 1.0) / av) / NxNy;
+		a.mean[u] = A * mean0[u] + B * Mk[u];
+		a.acc[u] = 0.0;
+	}
+}
+
+// x-pass STEP: Y tile -> (Hermitian pairs) -> inverse FFT, its last pass into
+// registers -> + mean, NaN check, NL, FP64 sum of NL -> forward FFT from
+// registers -> unpack -> Z tile. U in {1, 2}; pair p holds row p (U = 2: the
+// two fields as real and imaginary part) or rows 2p, 2p + 1 (U = 1).
+template <typename T, int U, int NC, int RC, int P, int NT, int MAXE>
+__device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm, const cplx<T>* tws, int tile, int tid) {
+	using PL = CtPlan<NC, MAXE>;
+	using RB = RegBlock<NC, MAXE, P, NT, T>;
+	constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
+	constexpr int H = NC / 2 + 1;
+	constexpr int CH = U * RC;
+	const long long tofs = (long long)tile * H * RC;
+	// Hermitian-extended pair spectra (as in the runtime kernel); the loop is
+	// unrolled so that all of a thread's loads are in flight together
+	constexpr int KIT = (H + NT - 1) / NT;
+#pragma unroll
+	for (int it = 0; it < KIT; it++) {
+		const int k = tid + it * NT;
+		if (k >= H) break;
+		cplx<T> y[CH];
+#pragma unroll
+		for (int c = 0; c < CH; c++) y[c] = a.work[(c % U) * a.wstride + tofs + (long long)k * RC + c / U];
+		const bool selfc = (k == 0) || (2 * k == NC);
+#pragma unroll
+		for (int p = 0; p < P; p++) {
+			cplx<T> A = y[2 * p], B = y[2 * p + 1];
+			if (selfc) { A.y = (T)0; B.y = (T)0; }
+			sm[p * LD + pad<T>(k)] = mk<T>(A.x - B.y, A.y + B.x);
+			if (k > 0 && 2 * k < NC) sm[p * LD + pad<T>(NC - k)] = mk<T>(A.x + B.y, B.x - A.y);
+		}
+	}
+	__syncthreads();
+	// inverse transform: all passes but the last in shared memory, the last into registers
+	ct_pass<NC, PL::radix(0), PL::ns(0), PL::twoff(0), P, NT, +1, T>(sm, tws, tid);
+	ct_middle<NC, MAXE, P, NT, +1, T>(sm, tws, tid);
+	RB rb;
+	ct_last_to_regs<NC, MAXE, P, NT, +1, T>(sm, tws, rb, tid);
+	// nonlinear term in registers, pfc-relax.c:1188-1209
+	T offT[U], lam[U], del[U], gam[U][U], alp[U][U];
+#pragma unroll
+	for (int u = 0; u < U; u++) {
+		offT[u] = (T)a.off[u];
+		lam[u] = (T)a.m.lambda[u];
+		del[u] = (T)a.m.delta[u];
+#pragma unroll
+		for (int v = 0; v < U; v++) { gam[u][v] = (T)a.m.gamma[u][v]; alp[u][v] = (T)a.m.alpha[u][v]; }
+	}
+	T accT[U];
+#pragma unroll
+	for (int u = 0; u < U; u++) accT[u] = (T)0;
+	bool nan = false;
+#pragma unroll
+	for (int i = 0; i < RB::NB; i++)
+#pragma unroll
+		for (int r = 0; r < MAXE; r++) {
+			cplx<T>& z = rb.v[i][r];
+			if constexpr (U == 2) {
+				const T m0 = z.x + offT[0], m1 = z.y + offT[1];
+				nan |= (m0 != m0) | (m1 != m1);
+				const T mc0 = alp[0][1] * m1 + (T)0.5 * gam[0][1] * ((T)2 * m0 * m1 + m1 * m1);
+				const T mc1 = alp[0][1] * m0 + (T)0.5 * gam[0][1] * ((T)2 * m1 * m0 + m0 * m0);
+				const T q0 = m0 * m0, q1 = m1 * m1;
+				const T nl0 = lam[0] + gam[0][0] * q0 + del[0] * m0 * q0 + mc0;
+				const T nl1 = lam[1] + gam[1][1] * q1 + del[1] * m1 * q1 + mc1;
+				accT[0] += nl0;
+				accT[1] += nl1;
+				z = mk<T>(nl0, nl1);
+			} else {
+				const T m0 = z.x + offT[0], m1 = z.y + offT[0];
+				nan |= (m0 != m0) | (m1 != m1);
+				const T q0 = m0 * m0, q1 = m1 * m1;
+				const T nl0 = lam[0] + gam[0][0] * q0 + del[0] * m0 * q0;
+				const T nl1 = lam[0] + gam[0][0] * q1 + del[0] * m1 * q1;
+				accT[0] += nl0 + nl1;
+				z = mk<T>(nl0, nl1);
+			}
+		}
+	// forward transform: first pass from registers, the rest in shared memory
+	ct_first_from_regs<NC, MAXE, P, NT, -1, T>(sm, rb, tid);
+	ct_middle<NC, MAXE, P, NT, -1, T>(sm, tws, tid);
+	ct_pass<NC, MAXE, PL::ns(PL::NPASS - 1), PL::twoff(PL::NPASS - 1), P, NT, -1, T>(sm, tws, tid);
+	if (nan) atomicOr(a.flag, 1);
+	// split the pairs and store the Z tile
+	const T half = (T)0.5;
+	for (int k = tid; k < H; k += NT) {
+		const int km = (k == 0) ? 0 : NC - k;
+		cplx<T> zz[2 * P];
+#pragma unroll
+		for (int p = 0; p < P; p++) {
+			const cplx<T> Ck = sm[p * LD + pad<T>(k)];
+			const cplx<T> Cm = sm[p * LD + pad<T>(km)];
+			zz[2 * p] = mk<T>(half * (Ck.x + Cm.x), half * (Ck.y - Cm.y));
+			zz[2 * p + 1] = mk<T>(half * (Ck.y + Cm.y), half * (Cm.x - Ck.x));
+		}
+#pragma unroll
+		for (int c = 0; c < CH; c++) a.work[(c % U) * a.wstride + tofs + (long long)k * RC + c / U] = zz[c];
+	}
+	double acc[U];
+#pragma unroll
+	for (int u = 0; u < U; u++) acc[u] = (double)accT[u];
+	block_reduce_add<U>(acc, a.acc);
+}
+
+// y-pass STEP: Z columns from global straight into the first forward pass ->
+// forward FFT, last pass into registers -> coupling + ETD1 update in registers
+// -> Hermitian fix of the kx = 0 and kx = Nx/2 columns (their CTAs only) ->
+// inverse FFT from registers, last pass into registers -> Y columns to global.
+// One butterfly of one field per thread, NT = U * CC * N/MAXE. With two fields
+// the PairMap puts them in lanes l and l ^ 16 at the same points: each thread
+// reads only its own field's spectral state and gets the other one by a
+// shuffle, so no thread reads an entry another thread writes.
+template <typename T, int U, int NC, int CCC, int RC, int S, int NT, int MAXE>
+__device__ __forceinline__ void ypass_step_fused(const YArgs<T>& a, cplx<T>* sm, const cplx<T>* tws, int kx0, int ncol,
+                                                 int tid) {
+	using MAP = typename std::conditional<U == 2, PairMap<NC, MAXE, CCC>, StdMap<NC, MAXE, S, NT>>::type;
+	using RB = RegBlock<NC, MAXE, S, NT, T, MAP>;
+	static_assert(RB::NB == 1 && NT == U * CCC * (NC / MAXE), "one butterfly per thread");
+	constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
+	constexpr int NR = NC / MAXE;
+	const int Nx = a.g.Nx, H = a.g.H;
+	const long long tileH = (long long)H * RC;
+	const int p = MAP::seq(tid, 0);
+	const int u = p / CCC, c = p % CCC;
+	const int j = MAP::bj(tid, 0);
+	const int kx = kx0 + c;
+	const bool live = c < ncol;
+	RB rb;
+	// Z column: element y at work[u][y / RC][kx][y % RC]
+	{
+		const cplx<T>* src = a.work + u * a.wstride + (long long)kx * RC;
+#pragma unroll
+		for (int r = 0; r < MAXE; r++) {
+			const int y = j + r * NR;
+			rb.v[0][r] = live ? src[(long long)(y / RC) * tileH + y % RC] : mk<T>((T)0, (T)0);
+		}
+	}
+	ct_first_from_regs<NC, MAXE, S, NT, -1, T, MAP>(sm, rb, tid);
+	ct_middle<NC, MAXE, S, NT, -1, T>(sm, tws, tid);
+	ct_last_to_regs<NC, MAXE, S, NT, -1, T, MAP>(sm, tws, rb, tid);
+
+	// update, pfc-relax.c:1215-1244 (A, B of update_AB, :901-958, recomputed);
+	// the field's own constants, selected once
+	const StepConsts<T, U> K(a.m, Nx, NC);
+	const T dkxT = (T)a.g.dkx, dkyT = (T)a.g.dky;
+	const T alpha = pick<T, U>(K.alpha, u), betad = pick<T, U>(K.betad, u);
+	const int W = pick<int, U>(K.W, u);
+	T nu2[MAXW], om[MAXW], ph[MAXW];
+#pragma unroll
+	for (int w = 0; w < MAXW; w++) {
+		nu2[w] = K.nu2[0][w];
+		om[w] = K.omega[0][w];
+		ph[w] = K.phi[0][w];
+		if constexpr (U > 1)
+			if (u == 1) { nu2[w] = K.nu2[1][w]; om[w] = K.omega[1][w]; ph[w] = K.phi[1][w]; }
+	}
+	// no store to the spectral state inside this loop, so the compiler may issue
+	// its loads as early as registers allow
+	const cplx<T>* spec_in = a.spec + u * a.sstride + (long long)kx * NC;
+#pragma unroll
+	for (int r = 0; r < MAXE; r++) {
+		const int ky = j + r * NR;
+		const cplx<T> Nown = live ? spec_in[ky] : mk<T>((T)0, (T)0);
+		const T k2 = k2_step<T>(kx, ky, NC, dkxT, dkyT);
+		cplx<T> M = cscale(rb.v[0][r], K.invN);
+		if constexpr (U > 1) {
+			cplx<T> Noth;
+			Noth.x = __shfl_xor_sync(0xffffffffu, Nown.x, 16);
+			Noth.y = __shfl_xor_sync(0xffffffffu, Nown.y, 16);
+			const T G = expT<T>(K.ag * k2);
+			T d2 = K.mu2[0][1] - k2;
+			d2 *= d2;
+			const T cu = K.beta[0][1] * d2 + K.eps[0][1] * G * G;
+			M = cadd(M, cscale(Noth, cu));
+		}
+		T Pk = (T)1;
+#pragma unroll
+		for (int w = 0; w < MAXW; w++)
+			if (w < W) {
+				const T q = nu2[w] - k2;
+				Pk *= om[w] * q * q + ph[w];
+			}
+		const T av = alpha + betad * Pk;
+		const T o = K.cc - (T)1 - K.cc * k2;
+		const T x = o * av * K.dt;
+		const T A = expT<T>(x);
+		T Bn;
+		if constexpr (sizeof(T) == 4) Bn = o * K.dt * phi1f(x, A);
+		else Bn = (av == (T)0) ? o * K.dt : etd_b<T>(A, x, av);
+		cplx<T> nn = cadd(cscale(Nown, A), cscale(M, Bn));
+		if (kx == 0 && ky == 0) nn = mk<T>((T)0, (T)0);
+		rb.v[0][r] = nn;
+	}
+	if (live) {
+		cplx<T>* spec_out = a.spec + u * a.sstride + (long long)kx * NC;
+#pragma unroll
+		for (int r = 0; r < MAXE; r++) spec_out[j + r * NR] = rb.v[0][r];
+	}
+	// kx = 0 and (even Nx) kx = Nx/2: Hermitian projection needs ky and -ky together
+	const int kn = (Nx % 2 == 0) ? Nx / 2 : -1;
+	const bool has0 = (kx0 == 0);
+	const bool hasn = (kn >= kx0 && kn < kx0 + ncol);
+	if (has0 || hasn) {
+		__syncthreads();
+#pragma unroll
+		for (int r = 0; r < MAXE; r++) sm[p * LD + pad<T>(j + r * NR)] = rb.v[0][r];
+		__syncthreads();
+#pragma unroll
+		for (int v = 0; v < U; v++) {
+			if (has0) hermitian_column<T>(sm + (v * CCC) * LD, a.spec + v * a.sstride, NC, tid, NT);
+			if (hasn)
+				hermitian_column<T>(sm + (v * CCC + (kn - kx0)) * LD, a.spec + v * a.sstride + (long long)kn * NC, NC, tid,
+				                    NT);
+		}
+#pragma unroll
+		for (int r = 0; r < MAXE; r++) rb.v[0][r] = sm[p * LD + pad<T>(j + r * NR)];
+	}
+	ct_first_from_regs<NC, MAXE, S, NT, +1, T, MAP>(sm, rb, tid);
+	ct_middle<NC, MAXE, S, NT, +1, T>(sm, tws, tid);
+	ct_last_to_regs<NC, MAXE, S, NT, +1, T, MAP>(sm, tws, rb, tid);
+	if (live) {
+		cplx<T>* dst = a.work + u * a.wstride + (long long)kx * RC;
+#pragma unroll
+		for (int r = 0; r < MAXE; r++) {
+			const int y = j + r * NR;
+			dst[(long long)(y / RC) * tileH + y % RC] = rb.v[0][r];
+		}
+	}
+	if (kx0 == 0 && tid == 0) ypass_mean_update<T, U>(a);
+}
 
 // ----------------------------------------------------------------- x-pass --
 
@@ -148,6 +491,11 @@ __global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MI
 	cplx<T>* tws = sm + (C::CT ? C::P * C::LD : 0);
 	if constexpr (C::CT) {
 		for (int i = tid; i < C::TWN; i += C::NT) tws[i] = a.twct[i];
+	}
+	if constexpr (MODE == XP_STEP && C::CT && CtPlan<NC, MAXE>::FUSABLE && C::NSUB == C::P && U <= 2 &&
+	              (U * RC) % 2 == 0) {
+		xpass_step_fused<T, U, NC, RC, C::P, C::NT, MAXE>(a, sm, tws, tile, tid);
+		return;
 	}
 
 	double off[U];
@@ -318,76 +666,12 @@ __global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MI
 
 // ----------------------------------------------------------------- y-pass --
 
-// Model constants of the k-space update converted once to the transform
-// precision (converting inside the per-entry loop costs an F2F per use).
-template <typename T, int U> struct StepConsts {
-	T invN, cc, dt, ag;
-	int W[U];
-	T alpha[U], betad[U];
-	T nu2[U][MAXW], omega[U][MAXW], phi[U][MAXW];
-	T beta[U][U], eps[U][U], mu2[U][U];
-	__device__ __forceinline__ StepConsts(const Model& m, int Nx, int Ny) {
-		invN = (T)(1.0 / ((double)Nx * (double)Ny));
-		cc = (T)m.c;
-		dt = (T)m.dt;
-		ag = (T)(-0.5 / m.sigma / m.sigma);
-#pragma unroll
-		for (int u = 0; u < U; u++) {
-			W[u] = m.W[u];
-			alpha[u] = (T)m.alpha[u][u];
-			betad[u] = (T)m.beta[u][u];
-#pragma unroll
-			for (int w = 0; w < MAXW; w++) {
-				nu2[u][w] = (T)m.nu2[u][w];
-				omega[u][w] = (T)m.omega[u][w];
-				phi[u][w] = (T)m.phi[u][w];
-			}
-#pragma unroll
-			for (int v = 0; v < U; v++) {
-				beta[u][v] = (T)m.beta[u][v];
-				eps[u][v] = (T)m.epsilon[u][v];
-				mu2[u][v] = (T)m.mu2[u][v];
-			}
-		}
-	}
-};
 
-// Hermitian projection of one resident column (kx = 0 or kx = Nx/2): entry ky
-// and entry Ny - ky become (a + conj b)/2 and its conjugate, self-conjugate
-// entries become real. Writes shared memory and the spectral state. This is
-// the reference's resynchronisation N^ = FFT(c2r(N^)) (pfc-relax.c:1179-1185)
-// restricted to the only columns where it is not the identity, done every
-// step: their anti-Hermitian part is invisible to c2r and is not acted on by
-// the nonlinear term, so between resyncs it grows like A(k)^t for every
-// unstable k (x1.28 per step for epsilon = -0.25, dt = 1), which overflows in FP32.
-template <typename T>
-__device__ __forceinline__ void hermitian_column(cplx<T>* col, cplx<T>* spec_col, int Ny, int tid, int nt) {
-	const int half = Ny / 2;
-	for (int base = 0; base <= half; base += nt) {
-		const int j = base + tid;
-		cplx<T> p = mk<T>((T)0, (T)0);
-		const int jn = (Ny - j) % Ny;
-		if (j <= half) {
-			const cplx<T> a = col[pad<T>(j)], b = col[pad<T>(jn)];
-			p = mk<T>((T)0.5 * (a.x + b.x), (T)0.5 * (a.y - b.y));
-		}
-		__syncthreads();
-		if (j <= half) {
-			col[pad<T>(j)] = p;
-			spec_col[j] = p;
-			if (jn != j) {
-				col[pad<T>(jn)] = cconj(p);
-				spec_col[jn] = cconj(p);
-			}
-		}
-		__syncthreads();
-	}
-}
 
-template <typename T, int U, int MODE, int NC, int CCC, int RC>
-__global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC>::NT, YCfg<T, U, NC, CCC, RC>::MINB)
+template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
+__global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC, FUSEDK>::NT, YCfg<T, U, NC, CCC, RC, FUSEDK>::MINB)
     ypass_kernel(const YArgs<T> a) {
-	using C = YCfg<T, U, NC, CCC, RC>;
+	using C = YCfg<T, U, NC, CCC, RC, FUSEDK>;
 	constexpr int MAXE = C::MAXE;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
@@ -409,16 +693,46 @@ __global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC>::NT, YCfg<T, U, NC, CC
 		for (int i = tid; i < C::TWN; i += C::NT) tws[i] = a.twct[i];
 	}
 
+	if constexpr (MODE == YP_STEP && C::FUSED && FUSEDK) {
+		ypass_step_fused<T, U, NC, CCC, RC, C::S, C::NT, MAXE>(a, sm, tws, kx0, ncol, tid);
+		return;
+	}
+
 	if constexpr (MODE != YP_WEIGHT) {
+		if constexpr (C::CT && ((NC / RC) * CCC * RC) % C::NT == 0) {
+			// every load of the tile in flight before the first shared-memory store
+			constexpr int CH = CCC * RC;
+			constexpr int PER = (NC / RC) * CH / C::NT;
+			cplx<T> v[U][PER];
 #pragma unroll
-		for (int u = 0; u < U; u++) {
-			const cplx<T>* src = a.work + u * a.wstride + (long long)kx0 * R;
-			for (int e = tid; e < ntile * chunk; e += nt) {
-				const int t = e / chunk, rem = e - t * chunk;
-				const int c = rem / R, r = rem - c * R;
-				cplx<T> v = mk<T>((T)0, (T)0);
-				if (c < ncol) v = src[t * tileH + rem];
-				sm[(u * CC + c) * ld + pad<T>(t * R + r)] = v;
+			for (int u = 0; u < U; u++) {
+				const cplx<T>* src = a.work + u * a.wstride + (long long)kx0 * RC;
+#pragma unroll
+				for (int i = 0; i < PER; i++) {
+					const int e = tid + i * C::NT;
+					const int t = e / CH, rem = e % CH;
+					v[u][i] = (rem / RC < ncol) ? src[t * tileH + rem] : mk<T>((T)0, (T)0);
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < U; u++)
+#pragma unroll
+				for (int i = 0; i < PER; i++) {
+					const int e = tid + i * C::NT;
+					const int t = e / CH, rem = e % CH;
+					sm[(u * CCC + rem / RC) * C::LD + pad<T>(t * RC + rem % RC)] = v[u][i];
+				}
+		} else {
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				const cplx<T>* src = a.work + u * a.wstride + (long long)kx0 * R;
+				for (int e = tid; e < ntile * chunk; e += nt) {
+					const int t = e / chunk, rem = e - t * chunk;
+					const int c = rem / R, r = rem - c * R;
+					cplx<T> v = mk<T>((T)0, (T)0);
+					if (c < ncol) v = src[t * tileH + rem];
+					sm[(u * CC + c) * ld + pad<T>(t * R + r)] = v;
+				}
 			}
 		}
 		__syncthreads();
@@ -504,32 +818,7 @@ __global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC>::NT, YCfg<T, U, NC, CC
 				update(c, kx, ky, Nv);
 			}
 		}
-		if (kx0 == 0 && tid == 0) {
-			// k = 0 in FP64: mean' = A(0) mean + B(0) (sum NL + couplings), pfc-relax.c:1215-1244 at k = 0
-			const double NxNy = (double)Nx * (double)Ny;
-			double mean0[U], Mk[U];
-#pragma unroll
-			for (int u = 0; u < U; u++) { mean0[u] = a.mean[u]; Mk[u] = a.acc[u]; }
-#pragma unroll
-			for (int u = 0; u < U - 1; u++)
-#pragma unroll
-				for (int v = u + 1; v < U; v++) {
-					const double d2 = a.m.mu2[u][v] * a.m.mu2[u][v];
-					const double cu = a.m.beta[u][v] * d2 + a.m.epsilon[u][v];
-					Mk[u] += cu * mean0[v] * NxNy;
-					Mk[v] += cu * mean0[u] * NxNy;
-				}
-#pragma unroll
-			for (int u = 0; u < U; u++) {
-				const double P0 = P_of<double>(a.m, u, 0.0);
-				const double av = a.m.alpha[u][u] + a.m.beta[u][u] * P0;
-				const double o = a.m.c - 1.0;
-				const double A = exp(o * av * a.m.dt);
-				const double B = ((av == 0.0) ? o * a.m.dt : (A - 1.0) / av) / NxNy;
-				a.mean[u] = A * mean0[u] + B * Mk[u];
-				a.acc[u] = 0.0;
-			}
-		}
+		if (kx0 == 0 && tid == 0) ypass_mean_update<T, U>(a);
 	} else if constexpr (MODE == YP_INIT) {
 		const T invN = (T)(1.0 / ((double)Nx * (double)Ny));
 		for (int e = tid; e < CC * Ny; e += nt) {
@@ -731,9 +1020,9 @@ template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, cons
 	return cudaErrorInvalidValue;
 }
 
-template <typename T, int U, int MODE, int NC, int CCC, int RC>
+template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
 static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
-	auto k = ypass_kernel<T, U, MODE, NC, CCC, RC>;
+	auto k = ypass_kernel<T, U, MODE, NC, CCC, RC, FUSEDK>;
 	static unsigned long long mask = 0;
 	smem_attr(k, mask);
 	k<<<c.grid, c.block, c.smem, s>>>(a);
@@ -741,10 +1030,15 @@ static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s
 }
 
 template <typename T, int U> static cudaError_t ystep(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
-	if (c.spec && y_is_spec<T, U, 4096>(a))
+	// c.spec: 1 = specialised (fused where possible), 2 = specialised, never fused
+	if (c.spec && y_is_spec<T, U, 4096>(a)) {
+		if (c.spec == 2) return ylaunch<T, U, YP_STEP, 4096, Spec<T>::ycc(U, 4096), Spec<T>::xr(U, 4096), false>(a, c, s);
 		return ylaunch<T, U, YP_STEP, 4096, Spec<T>::ycc(U, 4096), Spec<T>::xr(U, 4096)>(a, c, s);
-	if (c.spec && y_is_spec<T, U, 2048>(a))
+	}
+	if (c.spec && y_is_spec<T, U, 2048>(a)) {
+		if (c.spec == 2) return ylaunch<T, U, YP_STEP, 2048, Spec<T>::ycc(U, 2048), Spec<T>::xr(U, 2048), false>(a, c, s);
 		return ylaunch<T, U, YP_STEP, 2048, Spec<T>::ycc(U, 2048), Spec<T>::xr(U, 2048)>(a, c, s);
+	}
 	return ylaunch<T, U, YP_STEP, 0, 0, 0>(a, c, s);
 }
 
