@@ -128,6 +128,32 @@ int pfcg_set_device(int device);
 int pfcg_set_profiling(pfcg_handle* h, int on);
 int pfcg_profile_read(pfcg_handle* h, double* ms, long long* launches, int nkinds);
 
+/* Measures the launch shapes the runtime-plan kernels can take for this
+ * handle's size (rows per x-pass tile, columns per y-pass group) over nsteps
+ * steps each and keeps the fastest; results are cached per (precision, U, Nx,
+ * Ny) for the process. Call before pfcg_upload: the timing steps run on the
+ * handle's buffers, which are cleared afterwards. Sizes with compile-time
+ * specialised kernels (2048, 4096) keep their fixed shape. No counterpart in
+ * the reference (FFTW_MEASURE planning, pfc-relax.c:227-231, is the nearest). */
+int pfcg_autotune(pfcg_handle* h, int nsteps);
+
+/* Many independent relaxations (sizes, fields and parameters may differ)
+ * stepped together: one step of all problems is two kernel launches (a batched
+ * x-pass and a batched y-pass over per-problem tables), and pfcg_batch_step
+ * captures nsteps of them into one CUDA graph (cached per nsteps) and launches
+ * it. Problem i is an ordinary handle (pfcg_batch_problem) for upload,
+ * evaluate, optimize and download; do not step it on its own while the batch is
+ * in use. params is an array of nprob structs; autotune != 0 runs
+ * pfcg_autotune on every problem first. No counterpart in the reference, which
+ * relaxes one system per process. */
+typedef struct pfcg_batch pfcg_batch;
+int pfcg_batch_create(int nprob, const pfcg_params* params, const int* Nx, const int* Ny, const double* dx,
+                      const double* dy, pfcg_prec prec, int autotune, pfcg_batch** out);
+pfcg_handle* pfcg_batch_problem(pfcg_batch* b, int i);
+int pfcg_batch_step(pfcg_batch* b, int nsteps); /* 39 if any problem saw a NaN */
+int pfcg_batch_launches(const pfcg_batch* b, int nsteps, long long* kernels, long long* graph_launches);
+void pfcg_batch_destroy(pfcg_batch* b);
+
 /* Bytes of the static device workspace of pfcg_relax_noalloc. */
 #define PFCG_NOALLOC_SCRATCH_BYTES (32u << 20)
 

@@ -13,8 +13,12 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -153,50 +157,34 @@ template <typename T> int padded_host(int n) { return padded_len<T>(n); }
 
 int padded(int n, bool fp64) { return fp64 ? padded_host<double>(n) : padded_host<float>(n); }
 
-// Chooses the row tile R (x-pass) and column group CC (y-pass): the largest
-// sizes that fit shared memory and still give at least two CTAs per SM.
-int choose_layout(pfcg_handle* h, int nsm) {
+bool x_tile_ok(const pfcg_handle* h, int r) {
+	const bool fp64 = h->prec == PFCG_FP64;
+	const size_t budget = fp64 ? 200 * 1024 : 150 * 1024;
+	if (h->Ny % r) return false;
+	const int CH = h->U * r;
+	if (CH > MAX_CH) return false;
+	const int P = (CH + 1) / 2;
+	if ((size_t)P * padded(h->Nx, fp64) * h->celem > budget) return false;
+	int nt;
+	return sub_batch(h->px, P, max_elems_per_thread(fp64), &nt) > 0;
+}
+
+bool y_group_ok(const pfcg_handle* h, int c) {
+	const bool fp64 = h->prec == PFCG_FP64;
+	const size_t budget = fp64 ? 200 * 1024 : 150 * 1024;
+	const int S = h->U * c;
+	if ((size_t)S * padded(h->Ny, fp64) * h->celem > budget) return false;
+	int nt;
+	return sub_batch(h->py, S, max_elems_per_thread(fp64), &nt) > 0;
+}
+
+// launch shapes of the runtime-plan kernels for row tile R and column group CC
+void set_generic_configs(pfcg_handle* h, int R, int CC) {
 	const bool fp64 = h->prec == PFCG_FP64;
 	const int maxe = max_elems_per_thread(fp64);
-	const size_t budget = fp64 ? 200 * 1024 : 150 * 1024;
-	const int want = 2 * nsm;
 	const int U = h->U;
-	int R = 0;
-	// the compile-time specialised STEP kernels fix the tile shape when the size has one
-	// PFCG_GENERIC_KERNELS=1 in the environment disables them (A/B checks)
-	const char* gen = std::getenv("PFCG_GENERIC_KERNELS");
-	const bool allow_spec = !(gen && gen[0] == '1');
-	const int rs = allow_spec ? spec_rows(fp64, U, h->Nx) : 0;
-	if (rs && h->Ny % rs == 0) R = rs;
-	for (int r : {8, 4, 2, 1}) {
-		if (R) break;
-		if (h->Ny % r) continue;
-		const int CH = U * r;
-		if (CH > MAX_CH) continue;
-		const int P = (CH + 1) / 2;
-		if ((size_t)P * padded(h->Nx, fp64) * h->celem > budget) continue;
-		int nt;
-		if (!sub_batch(h->px, P, maxe, &nt)) continue;
-		R = r;
-		if (h->Ny / r >= want) break;
-	}
-	if (!R) return fail(h, PFCG_ESIZE, "no x-pass tile fits shared memory for this Nx");
-	int CC = 0;
-	const bool yspec = allow_spec && spec_cols(fp64, U, h->Ny) && spec_rows(fp64, U, h->Ny) == R;
-	if (yspec) CC = spec_cols(fp64, U, h->Ny);
-	for (int c : {4, 2, 1}) {
-		if (CC) break;
-		const int S = U * c;
-		if ((size_t)S * padded(h->Ny, fp64) * h->celem > budget) continue;
-		int nt;
-		if (!sub_batch(h->py, S, maxe, &nt)) continue;
-		CC = c;
-		if ((h->H + c - 1) / c >= want) break;
-	}
-	if (!CC) return fail(h, PFCG_ESIZE, "no y-pass column group fits shared memory for this Ny");
 	h->geom.R = R;
 	h->geom.CC = CC;
-
 	int nt;
 	const int P = (U * R + 1) / 2;
 	h->sbx = sub_batch(h->px, P, maxe, &nt);
@@ -211,6 +199,40 @@ int choose_layout(pfcg_handle* h, int nsm) {
 	h->cy1 = {(h->H + CC - 1) / CC, nt, (int)(CC * padded(h->Ny, fp64) * h->celem)};
 	h->cxs = h->cx;
 	h->cys = h->cy;
+}
+
+// Chooses the row tile R (x-pass) and column group CC (y-pass): the shape of
+// the compile-time specialised kernels where the size has one, otherwise the
+// largest sizes that fit shared memory and still give two CTAs per SM
+// (pfcg_autotune can replace this guess by measurement).
+int choose_layout(pfcg_handle* h, int nsm) {
+	const bool fp64 = h->prec == PFCG_FP64;
+	const int want = 2 * nsm;
+	const int U = h->U;
+	int R = 0;
+	// PFCG_GENERIC_KERNELS=1 in the environment disables the specialised kernels (A/B checks)
+	const char* gen = std::getenv("PFCG_GENERIC_KERNELS");
+	const bool allow_spec = !(gen && gen[0] == '1');
+	const int rs = allow_spec ? spec_rows(fp64, U, h->Nx) : 0;
+	if (rs && h->Ny % rs == 0) R = rs;
+	for (int r : {8, 4, 2, 1}) {
+		if (R) break;
+		if (!x_tile_ok(h, r)) continue;
+		R = r;
+		if (h->Ny / r >= want) break;
+	}
+	if (!R) return fail(h, PFCG_ESIZE, "no x-pass tile fits shared memory for this Nx");
+	int CC = 0;
+	const bool yspec = allow_spec && spec_cols(fp64, U, h->Ny) && spec_rows(fp64, U, h->Ny) == R;
+	if (yspec) CC = spec_cols(fp64, U, h->Ny);
+	for (int c : {4, 2, 1}) {
+		if (CC) break;
+		if (!y_group_ok(h, c)) continue;
+		CC = c;
+		if ((h->H + c - 1) / c >= want) break;
+	}
+	if (!CC) return fail(h, PFCG_ESIZE, "no y-pass column group fits shared memory for this Ny");
+	set_generic_configs(h, R, CC);
 	if (rs && R == rs) h->cxs = {h->Ny / R, spec_x_threads(fp64, U, h->Nx), spec_x_smem(fp64, U, h->Nx), 1};
 	if (yspec) {
 		// The specialised y-pass keeps the update between the two transforms in
@@ -812,6 +834,267 @@ int pfcg_launch_count(const pfcg_handle* h, long long* count) {
 }
 
 const char* pfcg_last_error(const pfcg_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+} // extern "C"
+
+// --------------------------------------------------------------- autotune ---
+namespace {
+
+// measured (R, CC) per (precision, U, Nx, Ny), shared by every handle of the process
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tune;
+
+template <typename T> int time_steps(pfcg_handle* h, int nsteps, float* ms) {
+	XArgs<T> xa = xargs<T>(h);
+	xa.acc = h->acc + ACC_NL;
+	YArgs<T> ya = yargs<T>(h);
+	cudaEvent_t e0, e1;
+	CK(h, cudaEventCreate(&e0));
+	CK(h, cudaEventCreate(&e1));
+	int rc = 0;
+	for (int s = 0; s < nsteps + 2 && !rc; s++) {
+		if (s == 2) cudaEventRecord(e0, h->stream);
+		rc = run_xpass<T>(h, XP_STEP, xa, h->cxs);
+		if (!rc) rc = run_ypass<T>(h, YP_STEP, ya, h->cys);
+	}
+	cudaEventRecord(e1, h->stream);
+	cudaEventSynchronize(e1);
+	cudaEventElapsedTime(ms, e0, e1);
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	return rc;
+}
+
+} // namespace
+
+extern "C" int pfcg_autotune(pfcg_handle* h, int nsteps) {
+	if (!h || nsteps < 1) return fail(h, PFCG_EARG, "bad argument");
+	if (h->cxs.spec || h->cys.spec) return 0; // the specialised kernels have a fixed shape
+	const auto key = std::make_tuple((int)h->prec, h->U, h->Nx, h->Ny);
+	{
+		std::lock_guard<std::mutex> lk(g_tune_mu);
+		auto it = g_tune.find(key);
+		if (it != g_tune.end()) {
+			set_generic_configs(h, it->second.first, it->second.second);
+			return 0;
+		}
+	}
+	float best = 1e30f;
+	int bR = h->geom.R, bC = h->geom.CC;
+	for (int r : {8, 4, 2, 1}) {
+		if (!x_tile_ok(h, r)) continue;
+		for (int c : {4, 2, 1}) {
+			if (!y_group_ok(h, c)) continue;
+			set_generic_configs(h, r, c);
+			float ms = 0.f;
+			const int rc = h->prec == PFCG_FP64 ? time_steps<double>(h, nsteps, &ms) : time_steps<float>(h, nsteps, &ms);
+			if (rc) return rc;
+			if (ms < best) { best = ms; bR = r; bC = c; }
+		}
+	}
+	set_generic_configs(h, bR, bC);
+	// the timing steps ran on whatever the buffers held: start clean
+	const size_t nspec = (size_t)h->H * h->Ny * h->U;
+	CK(h, cudaMemsetAsync(h->spec, 0, h->celem * nspec, h->stream));
+	CK(h, cudaMemsetAsync(h->work, 0, h->celem * nspec, h->stream));
+	CK(h, cudaMemsetAsync(h->mean, 0, sizeof(double) * MAXU, h->stream));
+	CK(h, cudaMemsetAsync(h->acc, 0, sizeof(double) * ACC_N, h->stream));
+	CK(h, cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+	CK(h, cudaStreamSynchronize(h->stream));
+	std::lock_guard<std::mutex> lk(g_tune_mu);
+	g_tune[key] = {bR, bC};
+	return 0;
+}
+
+// ------------------------------------------------------------------ batch ---
+struct pfcg_batch {
+	pfcg_prec prec = PFCG_FP32;
+	std::vector<pfcg_handle*> h;
+	cudaStream_t stream = nullptr;
+	void* d_xargs = nullptr;
+	void* d_yargs = nullptr;
+	int* d_blk = nullptr; // x problem, x local, y problem, y local tables
+	int* d_flags = nullptr;
+	int* h_flags = nullptr;
+	int xblocks = 0, yblocks = 0, threads = 0, smem = 0;
+	std::map<int, cudaGraphExec_t> graphs;
+	std::string err;
+};
+
+namespace {
+
+template <typename T> int batch_build(pfcg_batch* b) {
+	const int n = (int)b->h.size();
+	std::vector<XArgs<T>> xa(n);
+	std::vector<YArgs<T>> ya(n);
+	// blocks of the largest problems first, so the tail of the launch is short
+	std::vector<int> order(n);
+	for (int i = 0; i < n; i++) order[i] = i;
+	std::sort(order.begin(), order.end(), [&](int a, int c) {
+		return (long long)b->h[a]->Nx * b->h[a]->Ny * b->h[a]->U > (long long)b->h[c]->Nx * b->h[c]->Ny * b->h[c]->U;
+	});
+	std::vector<int> xp, xl, yp, yl;
+	b->threads = 32;
+	b->smem = 0;
+	for (int i = 0; i < n; i++) {
+		pfcg_handle* h = b->h[i];
+		xa[i] = xargs<T>(h);
+		xa[i].acc = h->acc + ACC_NL;
+		xa[i].flag = b->d_flags + i;
+		ya[i] = yargs<T>(h);
+		b->threads = std::max(b->threads, std::max(h->cx.block, h->cy.block));
+		b->smem = std::max(b->smem, std::max(h->cx.smem, h->cy.smem));
+	}
+	for (int i : order) {
+		for (int t = 0; t < b->h[i]->cx.grid; t++) { xp.push_back(i); xl.push_back(t); }
+		for (int g = 0; g < b->h[i]->cy.grid; g++) { yp.push_back(i); yl.push_back(g); }
+	}
+	b->xblocks = (int)xp.size();
+	b->yblocks = (int)yp.size();
+	pfcg_handle* h0 = b->h[0];
+	auto bfail = [&](cudaError_t e, const char* what) {
+		b->err = std::string(what) + ": " + cudaGetErrorString(e);
+		return PFCG_ECUDA;
+	};
+	cudaError_t e;
+	if ((e = cudaMalloc(&b->d_xargs, sizeof(XArgs<T>) * n)) != cudaSuccess) return bfail(e, "cudaMalloc");
+	if ((e = cudaMalloc(&b->d_yargs, sizeof(YArgs<T>) * n)) != cudaSuccess) return bfail(e, "cudaMalloc");
+	if ((e = cudaMalloc(&b->d_blk, sizeof(int) * (2 * xp.size() + 2 * yp.size()))) != cudaSuccess) return bfail(e, "cudaMalloc");
+	cudaMemcpy(b->d_xargs, xa.data(), sizeof(XArgs<T>) * n, cudaMemcpyHostToDevice);
+	cudaMemcpy(b->d_yargs, ya.data(), sizeof(YArgs<T>) * n, cudaMemcpyHostToDevice);
+	int* q = b->d_blk;
+	cudaMemcpy(q, xp.data(), sizeof(int) * xp.size(), cudaMemcpyHostToDevice);
+	cudaMemcpy(q + xp.size(), xl.data(), sizeof(int) * xl.size(), cudaMemcpyHostToDevice);
+	cudaMemcpy(q + 2 * xp.size(), yp.data(), sizeof(int) * yp.size(), cudaMemcpyHostToDevice);
+	if ((e = cudaMemcpy(q + 2 * xp.size() + yp.size(), yl.data(), sizeof(int) * yl.size(), cudaMemcpyHostToDevice)) !=
+	    cudaSuccess)
+		return bfail(e, "cudaMemcpy");
+	(void)h0;
+	return 0;
+}
+
+template <typename T> int batch_launch_steps(pfcg_batch* b, int nsteps) {
+	const int* q = b->d_blk;
+	const int* xp = q;
+	const int* xl = q + b->xblocks;
+	const int* yp = q + 2 * b->xblocks;
+	const int* yl = yp + b->yblocks;
+	for (int s = 0; s < nsteps; s++) {
+		cudaError_t e = launch_batch_step<T>((const XArgs<T>*)b->d_xargs, (const YArgs<T>*)b->d_yargs, xp, xl, b->xblocks, yp,
+		                                     yl, b->yblocks, b->threads, b->smem, b->stream);
+		if (e != cudaSuccess) {
+			b->err = std::string("batch step: ") + cudaGetErrorString(e);
+			return PFCG_ECUDA;
+		}
+	}
+	return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int pfcg_batch_create(int nprob, const pfcg_params* params, const int* Nx, const int* Ny, const double* dx,
+                      const double* dy, pfcg_prec prec, int autotune, pfcg_batch** out) {
+	if (!out || nprob < 1 || !params || !Nx || !Ny || !dx || !dy) return fail(nullptr, PFCG_EARG, "bad argument");
+	*out = nullptr;
+	pfcg_batch* b = new pfcg_batch();
+	b->prec = prec;
+	auto bail = [&](int rc) {
+		if (!b->err.empty()) g_err = b->err;
+		pfcg_batch_destroy(b);
+		return rc;
+	};
+	for (int i = 0; i < nprob; i++) {
+		pfcg_handle* h = nullptr;
+		const int rc = pfcg_create(&params[i], Nx[i], Ny[i], dx[i], dy[i], prec, &h);
+		if (rc) return bail(rc);
+		b->h.push_back(h);
+		// the batch runs the runtime-plan kernels for every size
+		h->cxs = h->cx;
+		h->cys = h->cy;
+		if (autotune) {
+			const int r2 = pfcg_autotune(h, 5);
+			if (r2) {
+				b->err = h->err;
+				return bail(r2);
+			}
+		}
+	}
+	cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+	if (e == cudaSuccess) e = cudaMalloc(&b->d_flags, sizeof(int) * nprob);
+	if (e == cudaSuccess) e = cudaMemset(b->d_flags, 0, sizeof(int) * nprob);
+	if (e == cudaSuccess) e = cudaMallocHost(&b->h_flags, sizeof(int) * nprob);
+	if (e != cudaSuccess) {
+		b->err = cudaGetErrorString(e);
+		return bail(PFCG_ECUDA);
+	}
+	const int rc = prec == PFCG_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+	if (rc) return bail(rc);
+	*out = b;
+	return 0;
+}
+
+pfcg_handle* pfcg_batch_problem(pfcg_batch* b, int i) {
+	if (!b || i < 0 || i >= (int)b->h.size()) return nullptr;
+	return b->h[i];
+}
+
+int pfcg_batch_step(pfcg_batch* b, int nsteps) {
+	if (!b || nsteps < 0) return fail(nullptr, PFCG_EARG, "bad argument");
+	if (nsteps == 0) return 0;
+	// every problem's own stream must be idle (uploads are synchronous)
+	auto it = b->graphs.find(nsteps);
+	if (it == b->graphs.end()) {
+		if (b->prec == PFCG_FP64) prepare_batch_kernels<double>();
+		else prepare_batch_kernels<float>();
+		cudaGraph_t g;
+		cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+		if (e != cudaSuccess) { b->err = cudaGetErrorString(e); g_err = b->err; return PFCG_ECUDA; }
+		const int rc = b->prec == PFCG_FP64 ? batch_launch_steps<double>(b, nsteps) : batch_launch_steps<float>(b, nsteps);
+		e = cudaStreamEndCapture(b->stream, &g);
+		if (rc) { g_err = b->err; return rc; }
+		if (e != cudaSuccess) { b->err = cudaGetErrorString(e); g_err = b->err; return PFCG_ECUDA; }
+		cudaGraphExec_t ge;
+		e = cudaGraphInstantiate(&ge, g, 0);
+		cudaGraphDestroy(g);
+		if (e != cudaSuccess) { b->err = cudaGetErrorString(e); g_err = b->err; return PFCG_ECUDA; }
+		it = b->graphs.emplace(nsteps, ge).first;
+	}
+	cudaError_t e = cudaGraphLaunch(it->second, b->stream);
+	const int n = (int)b->h.size();
+	if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_flags, b->d_flags, sizeof(int) * n, cudaMemcpyDeviceToHost, b->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+	if (e != cudaSuccess) { b->err = cudaGetErrorString(e); g_err = b->err; return PFCG_ECUDA; }
+	for (pfcg_handle* h : b->h) {
+		h->t += nsteps;
+		h->launches += 2 * nsteps;
+	}
+	for (int i = 0; i < n; i++)
+		if (b->h_flags[i]) { g_err = "Not a number value detected."; return PFCG_NAN; }
+	return 0;
+}
+
+int pfcg_batch_launches(const pfcg_batch* b, int nsteps, long long* kernels, long long* graph_launches) {
+	if (!b) return PFCG_EARG;
+	if (kernels) *kernels = 2LL * nsteps;
+	if (graph_launches) *graph_launches = 1;
+	return 0;
+}
+
+void pfcg_batch_destroy(pfcg_batch* b) {
+	if (!b) return;
+	if (b->stream) cudaStreamSynchronize(b->stream);
+	for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+	for (pfcg_handle* h : b->h) pfcg_destroy(h);
+	cudaFree(b->d_xargs);
+	cudaFree(b->d_yargs);
+	cudaFree(b->d_blk);
+	cudaFree(b->d_flags);
+	if (b->h_flags) cudaFreeHost(b->h_flags);
+	if (b->stream) cudaStreamDestroy(b->stream);
+	delete b;
+}
 
 } // extern "C"
 

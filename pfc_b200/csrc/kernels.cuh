@@ -116,6 +116,14 @@ int spec_twiddles(bool fp64, int N);
 template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
 template <typename T> cudaError_t launch_ypass(int mode, const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
 
+// One step of many problems: the batched x-pass and y-pass kernels over
+// per-problem arguments in device memory and per-block (problem, tile) tables.
+template <typename T> void prepare_batch_kernels();
+template <typename T>
+cudaError_t launch_batch_step(const XArgs<T>* xprobs, const YArgs<T>* yprobs, const int* xblk_prob, const int* xblk_local,
+                              int xblocks, const int* yblk_prob, const int* yblk_local, int yblocks, int threads, int smem,
+                              cudaStream_t s);
+
 // Parseval sums for up to MAX_TRIAL box sizes (see kernels.cu): out[t] += ...
 template <typename T>
 cudaError_t launch_kspace_energy(const cplx<T>* spec, long long sstride, const Model& m, const Geom& g, int ntrial,

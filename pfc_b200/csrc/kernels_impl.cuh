@@ -470,8 +470,10 @@ __device__ __forceinline__ void ypass_step_fused(const YArgs<T>& a, cplx<T>* sm,
 
 // ----------------------------------------------------------------- x-pass --
 
+// Body of the x-pass for row tile `tile`; called by xpass_kernel (one problem)
+// and by xpass_batch_kernel (many problems in one launch).
 template <typename T, int U, int MODE, int NC, int RC>
-__global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MINB) xpass_kernel(const XArgs<T> a) {
+__device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile) {
 	using C = XCfg<T, U, NC, RC>;
 	constexpr int MAXE = C::MAXE;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -483,7 +485,6 @@ __global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MI
 	const int CH = U * R;
 	const int P = (CH + 1) >> 1;
 	const int ld = C::CT ? C::LD : padded_len<T>(Nx);
-	const int tile = blockIdx.x;
 	const int y0 = tile * R;
 	const int tid = threadIdx.x;
 	const int nt = C::CT ? C::NT : (int)blockDim.x;
@@ -668,9 +669,15 @@ __global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MI
 
 
 
+template <typename T, int U, int MODE, int NC, int RC>
+__global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MINB) xpass_kernel(const XArgs<T> a) {
+	xpass_body<T, U, MODE, NC, RC>(a, blockIdx.x);
+}
+
+// Body of the y-pass for column group `grp`; called by ypass_kernel and by
+// ypass_batch_kernel.
 template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
-__global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC, FUSEDK>::NT, YCfg<T, U, NC, CCC, RC, FUSEDK>::MINB)
-    ypass_kernel(const YArgs<T> a) {
+__device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 	using C = YCfg<T, U, NC, CCC, RC, FUSEDK>;
 	constexpr int MAXE = C::MAXE;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -681,7 +688,7 @@ __global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC, FUSEDK>::NT, YCfg<T, U
 	const int CC = C::CT ? CCC : a.g.CC;
 	const int S = U * CC;
 	const int ld = C::CT ? C::LD : padded_len<T>(Ny);
-	const int kx0 = blockIdx.x * CC;
+	const int kx0 = grp * CC;
 	const int ncol = min(CC, H - kx0);
 	const int ntile = Ny / R;
 	const long long tileH = (long long)H * R;
@@ -950,6 +957,46 @@ __global__ void __launch_bounds__(256) kspace_energy_kernel(const cplx<T>* __res
 
 // -------------------------------------------------------------- launchers --
 
+template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
+__global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC, FUSEDK>::NT, YCfg<T, U, NC, CCC, RC, FUSEDK>::MINB)
+    ypass_kernel(const YArgs<T> a) {
+	ypass_body<T, U, MODE, NC, CCC, RC, FUSEDK>(a, blockIdx.x);
+}
+
+// ------------------------------------------------------------------ batch --
+// Many independent relaxations of runtime sizes in one launch: block b runs
+// tile (x-pass) or column group (y-pass) blk_local[b] of problem blk_prob[b],
+// whose arguments sit in global memory. Launched with the largest thread count
+// and shared memory any problem needs; the runtime-plan bodies use whatever
+// threads they get.
+template <typename T>
+__global__ void __launch_bounds__(MAXNT, 1)
+    xpass_batch_kernel(const XArgs<T>* __restrict__ probs, const int* __restrict__ blk_prob,
+                       const int* __restrict__ blk_local) {
+	const XArgs<T>& a = probs[blk_prob[blockIdx.x]];
+	const int local = blk_local[blockIdx.x];
+	switch (a.m.U) {
+	case 1: xpass_body<T, 1, XP_STEP, 0, 0>(a, local); break;
+	case 2: xpass_body<T, 2, XP_STEP, 0, 0>(a, local); break;
+	case 3: xpass_body<T, 3, XP_STEP, 0, 0>(a, local); break;
+	case 4: xpass_body<T, 4, XP_STEP, 0, 0>(a, local); break;
+	}
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MAXNT, 1)
+    ypass_batch_kernel(const YArgs<T>* __restrict__ probs, const int* __restrict__ blk_prob,
+                       const int* __restrict__ blk_local) {
+	const YArgs<T>& a = probs[blk_prob[blockIdx.x]];
+	const int local = blk_local[blockIdx.x];
+	switch (a.m.U) {
+	case 1: ypass_body<T, 1, YP_STEP, 0, 0, 0>(a, local); break;
+	case 2: ypass_body<T, 2, YP_STEP, 0, 0, 0>(a, local); break;
+	case 3: ypass_body<T, 3, YP_STEP, 0, 0, 0>(a, local); break;
+	case 4: ypass_body<T, 4, YP_STEP, 0, 0, 0>(a, local); break;
+	}
+}
+
 // Raises the dynamic shared-memory limit of a kernel once per device.
 template <typename K> static void smem_attr(K k, unsigned long long& mask) {
 	int dev = 0;
@@ -1061,6 +1108,24 @@ template <typename T> cudaError_t launch_ypass(int mode, const YArgs<T>& a, cons
 		}
 	}
 	return cudaErrorInvalidValue;
+}
+
+template <typename T> void prepare_batch_kernels() {
+	static unsigned long long mx = 0, my = 0;
+	smem_attr(xpass_batch_kernel<T>, mx);
+	smem_attr(ypass_batch_kernel<T>, my);
+}
+
+template <typename T>
+cudaError_t launch_batch_step(const XArgs<T>* xprobs, const YArgs<T>* yprobs, const int* xblk_prob, const int* xblk_local,
+                              int xblocks, const int* yblk_prob, const int* yblk_local, int yblocks, int threads, int smem,
+                              cudaStream_t s) {
+	prepare_batch_kernels<T>();
+	xpass_batch_kernel<T><<<xblocks, threads, smem, s>>>(xprobs, xblk_prob, xblk_local);
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess) return e;
+	ypass_batch_kernel<T><<<yblocks, threads, smem, s>>>(yprobs, yblk_prob, yblk_local);
+	return cudaGetLastError();
 }
 
 template <typename T>

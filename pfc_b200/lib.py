@@ -46,6 +46,15 @@ SIGNATURES = {
     "pfcg_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _ip]),
     "pfcg_relax_noalloc": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_double, ctypes.c_double, _ip,
                                           ctypes.c_void_p, ctypes.c_void_p]),
+    "pfcg_autotune": (ctypes.c_int, [_vp, _ip]),
+    "pfcg_batch_create": (ctypes.c_int, [_ip, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_int), _dp, _dp, _ip, _ip,
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "pfcg_batch_problem": (ctypes.c_void_p, [_vp, _ip]),
+    "pfcg_batch_step": (ctypes.c_int, [_vp, _ip]),
+    "pfcg_batch_launches": (ctypes.c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_longlong),
+                                           ctypes.POINTER(ctypes.c_longlong)]),
+    "pfcg_batch_destroy": (None, [_vp]),
     "pfcg_stream": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
     "pfcg_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "pfcg_last_error": (ctypes.c_char_p, [_vp]),
@@ -185,6 +194,10 @@ class Relaxation:
         self._check(self.L.pfcg_stream(self.h, ctypes.byref(s)))
         return s.value or 0
 
+    def autotune(self, nsteps: int = 5) -> None:
+        """Measure the runtime-plan launch shapes and keep the fastest (before upload)."""
+        self._check(self.L.pfcg_autotune(self.h, nsteps))
+
     def set_profiling(self, on: bool) -> None:
         self._check(self.L.pfcg_set_profiling(self.h, 1 if on else 0))
 
@@ -239,3 +252,66 @@ def relax_noalloc(params: Params, Nx: int, Ny: int, dx: float, dy: float, nsteps
 
 def last_error() -> str:
     return load().pfcg_last_error(None).decode()
+
+
+class _Problem(Relaxation):
+    """A problem owned by a Batch: an ordinary handle that the batch frees."""
+
+    def __init__(self, L, h, params, Nx, Ny, precision):
+        self.L = L
+        self.h = ctypes.c_void_p(h)
+        self.params = params
+        self.U = params.U
+        self.Nx, self.Ny = Nx, Ny
+        self.precision = precision
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Many relaxations stepped together (pfcg_batch_*): one CUDA graph per step
+    count, two batched kernels per step."""
+
+    def __init__(self, problems, precision: str = "fp32", autotune: bool = True):
+        """problems: list of (Params, Nx, Ny, dx, dy)."""
+        self.L = load()
+        n = len(problems)
+        arr = (Params * n)(*[p[0] for p in problems])
+        Nx = (ctypes.c_int * n)(*[p[1] for p in problems])
+        Ny = (ctypes.c_int * n)(*[p[2] for p in problems])
+        dx = np.array([p[3] for p in problems], dtype=np.float64)
+        dy = np.array([p[4] for p in problems], dtype=np.float64)
+        b = ctypes.c_void_p()
+        rc = self.L.pfcg_batch_create(n, arr, Nx, Ny, _dptr(dx), _dptr(dy), {"fp32": FP32, "fp64": FP64}[precision],
+                                      1 if autotune else 0, ctypes.byref(b))
+        if rc:
+            raise PfcError(rc, self.L.pfcg_last_error(None).decode())
+        self.b = b
+        self.problems = [_Problem(self.L, self.L.pfcg_batch_problem(b, i), p[0], p[1], p[2], precision)
+                         for i, p in enumerate(problems)]
+
+    def step(self, n: int = 1) -> int:
+        rc = self.L.pfcg_batch_step(self.b, n)
+        if rc:
+            raise PfcError(rc, self.L.pfcg_last_error(None).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "b", None):
+            for p in self.problems:
+                p.close()
+            self.L.pfcg_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
