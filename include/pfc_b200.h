@@ -88,6 +88,34 @@ int pfcg_upload(pfcg_handle* h, const double* fields);
  * write_data prints (:803-809). */
 int pfcg_download(pfcg_handle* h, double* fields);
 
+/* As pfcg_upload / pfcg_download, with the fields in DEVICE memory (for data
+ * that is generated or consumed on the GPU). */
+int pfcg_upload_device(pfcg_handle* h, const double* d_fields);
+int pfcg_download_device(pfcg_handle* h, double* d_fields);
+
+/* Seeded two-field heterostructure initial state, generated on the device
+ * (the one-mode approximation and periodic Voronoi grains of the reference's
+ * initial-state builder, src/PFCInit.java:46-93 and :389-462). Each region
+ * belongs to one field, which carries mean[u] + amp[u] * OMA(r, sym,
+ * lattice[u]) there, rotated by the grain's angle; the other field sits at its
+ * mean. grains > 0: Voronoi grains with centres, angles in [0, max_angle_deg)
+ * and fields drawn from the seed; grains <= 0: vertical stripes of
+ * stripe_width columns, shifted by stripe_offset >= 0 columns, field
+ * ((x + offset) / width) % 2, unrotated. noise * N(0, 1) is added to both
+ * fields. d_fields: DEVICE, 2 x Ny x Nx doubles. No counterpart in the
+ * reference's C code (its states come from pfc-init.jar). */
+typedef struct pfcg_hetero {
+	int grains;
+	int stripe_width, stripe_offset;
+	int sym; /* 3 triangular, 4 square, 6 honeycomb */
+	double mean[2], amp[2], lattice[2];
+	double noise;
+	double max_angle_deg;
+	unsigned seed;
+} pfcg_hetero;
+int pfcg_init_hetero(double* d_fields, int Nx, int Ny, double dx, double dy, const pfcg_hetero* s, void* stream);
+const char* pfcg_init_last_error(void);
+
 /* Sets the grid spacing and rebuilds the linear operators. Replaces update_AB
  * (:901-958) after a change of s->dx, s->dy. */
 int pfcg_set_box(pfcg_handle* h, double dx, double dy);
@@ -153,6 +181,50 @@ pfcg_handle* pfcg_batch_problem(pfcg_batch* b, int i);
 int pfcg_batch_step(pfcg_batch* b, int nsteps); /* 39 if any problem saw a NaN */
 int pfcg_batch_launches(const pfcg_batch* b, int nsteps, long long* kernels, long long* graph_launches);
 void pfcg_batch_destroy(pfcg_batch* b);
+
+/* ---- Learned warm start. No counterpart in the reference. ----
+ * A Fourier neural operator on T x T periodic tiles of two fields (T a power
+ * of two in [32, 512]): a per-point lift of the two fields to C channels, L
+ * layers z = W v + b + K v (K: complex C x C weights on the retained Fourier
+ * modes kx = 0..MODES_X-1, ky = -MODES_Y/2..MODES_Y/2-1 of the tile; GELU after
+ * every layer but the last), and a per-point projection whose output is added
+ * to the input fields. Kernels read BF16 weights and accumulate in FP32; the
+ * FP32 master weights are what set/get_params and Adam see.
+ * Parameter layout (floats): P[C][2], p[C]; per layer W[C][C], b[C],
+ * Re R[C][C][MODES_Y][MODES_X], Im R[...] (R indexed [in][out][ky row][kx],
+ * ky rows 0..MODES_Y/2-1 = ky 0.., the rest = ky -MODES_Y/2..-1); Q[2][C], q[2]. */
+#define PFCG_FNO_LAYERS 4
+#define PFCG_FNO_CHANNELS 32
+#define PFCG_FNO_MODES_X 8
+#define PFCG_FNO_MODES_Y 16
+#define PFCG_FNO_PARAMS 1052962
+typedef struct pfcg_fno pfcg_fno;
+size_t pfcg_fno_param_count(void);
+/* max_batch tiles per launch sequence; memory grows as max_batch * T^2 * 1.9 KB. */
+int pfcg_fno_create(int tile, int max_batch, pfcg_fno** out);
+int pfcg_fno_set_params(pfcg_fno* f, const float* host_params); /* also resets Adam */
+int pfcg_fno_get_params(pfcg_fno* f, float* host_params);
+/* DEVICE tensors [batch][2][T][T] FP32 (x-fastest). */
+int pfcg_fno_forward(pfcg_fno* f, const float* d_in, float* d_out, int batch);
+/* Mean-square error of the output against d_target over all batch points and
+ * both fields, and its gradient (kept on the device for pfcg_fno_adam_step;
+ * copied to host_grad when it is not NULL). */
+int pfcg_fno_loss_grad(pfcg_fno* f, const float* d_in, const float* d_target, int batch, double* loss,
+                       float* host_grad);
+int pfcg_fno_adam_step(pfcg_fno* f, float lr, float beta1, float beta2, float eps);
+/* The network on a periodic DEVICE grid of two FP64 fields (2 x Ny x Nx,
+ * d_in != d_out): tiles of T points whose central T/2 x T/2 block is kept
+ * (T/4 points of periodic halo on each side); each field's mean is then
+ * restored to the input's in FP64, since the relaxation conserves it.
+ * stream: cudaStream_t the call is ordered on (NULL = default stream). */
+int pfcg_fno_apply(pfcg_fno* f, const double* d_in, double* d_out, int Nx, int Ny, void* stream);
+/* Replaces the handle's fields (U = 2) by the network's proposal, in place on
+ * the device; the step count is kept. */
+int pfcg_warmstart(pfcg_handle* h, pfcg_fno* f);
+int pfcg_fno_stream(const pfcg_fno* f, void** stream);
+int pfcg_fno_launch_count(const pfcg_fno* f, long long* count);
+const char* pfcg_fno_last_error(const pfcg_fno* f); /* NULL: last failed create */
+void pfcg_fno_destroy(pfcg_fno* f);
 
 /* Bytes of the static device workspace of pfcg_relax_noalloc. */
 #define PFCG_NOALLOC_SCRATCH_BYTES (32u << 20)

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/pfc_b200.h"
+#include "fno.cuh"
 #include "kernels.cuh"
 
 using namespace pfcg;
@@ -425,11 +426,11 @@ template <typename T> int run_ypass(pfcg_handle* h, int mode, const YArgs<T>& a,
 	return 0;
 }
 
-template <typename T> int do_upload(pfcg_handle* h, const double* fields) {
-	int rc = ensure_real(h);
-	if (rc) return rc;
+// Spectral state from the real fields in d_real (device): FP64 means, then the
+// forward transforms of the fluctuations.
+template <typename T> int spectral_from_real(pfcg_handle* h) {
 	const size_t npts = (size_t)h->Nx * h->Ny;
-	CK(h, cudaMemcpyAsync(h->d_real, fields, sizeof(double) * h->U * npts, cudaMemcpyHostToDevice, h->stream));
+	int rc = 0;
 	// the mean (k = 0 mode) in FP64, by a fixed-order reduction on the device
 	h->launches += 2;
 	{
@@ -443,18 +444,41 @@ template <typename T> int do_upload(pfcg_handle* h, const double* fields) {
 	rc = run_ypass<T>(h, YP_INIT, ya, h->cy);
 	if (rc) return rc;
 	CK(h, cudaStreamSynchronize(h->stream));
+	return 0;
+}
+
+template <typename T> int do_upload(pfcg_handle* h, const double* fields, cudaMemcpyKind kind) {
+	int rc = ensure_real(h);
+	if (rc) return rc;
+	CK(h, cudaMemcpyAsync(h->d_real, fields, sizeof(double) * h->U * (size_t)h->Nx * h->Ny, kind, h->stream));
+	rc = spectral_from_real<T>(h);
+	if (rc) return rc;
 	h->t = 0;
 	return 0;
 }
 
-template <typename T> int do_download(pfcg_handle* h, double* fields) {
+// Real fields -> network proposal -> spectral state, all on the device.
+template <typename T> int do_warmstart(pfcg_handle* h, pfcg_fno* f) {
 	int rc = ensure_real(h);
 	if (rc) return rc;
 	XArgs<T> xa = xargs<T>(h);
 	rc = run_xpass<T>(h, XP_C2R, xa, h->cx);
 	if (rc) return rc;
-	CK(h, cudaMemcpyAsync(fields, h->d_real, sizeof(double) * h->U * (size_t)h->Nx * h->Ny, cudaMemcpyDeviceToHost,
-	                      h->stream));
+	const size_t n = 2 * (size_t)h->Nx * h->Ny;
+	double* tmp = nullptr;
+	if (fno_scratch_grid(f, n, &tmp) || fno_apply_device(f, h->d_real, tmp, h->Nx, h->Ny, h->stream))
+		return fail(h, PFCG_ECUDA, std::string("warm start: ") + fno_error(f));
+	CK(h, cudaMemcpyAsync(h->d_real, tmp, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+	return spectral_from_real<T>(h);
+}
+
+template <typename T> int do_download(pfcg_handle* h, double* fields, cudaMemcpyKind kind) {
+	int rc = ensure_real(h);
+	if (rc) return rc;
+	XArgs<T> xa = xargs<T>(h);
+	rc = run_xpass<T>(h, XP_C2R, xa, h->cx);
+	if (rc) return rc;
+	CK(h, cudaMemcpyAsync(fields, h->d_real, sizeof(double) * h->U * (size_t)h->Nx * h->Ny, kind, h->stream));
 	CK(h, cudaStreamSynchronize(h->stream));
 	return 0;
 }
@@ -746,12 +770,32 @@ void pfcg_destroy(pfcg_handle* h) {
 
 int pfcg_upload(pfcg_handle* h, const double* fields) {
 	if (!h || !fields) return fail(h, PFCG_EARG, "NULL argument");
-	return h->prec == PFCG_FP64 ? do_upload<double>(h, fields) : do_upload<float>(h, fields);
+	return h->prec == PFCG_FP64 ? do_upload<double>(h, fields, cudaMemcpyHostToDevice)
+	                            : do_upload<float>(h, fields, cudaMemcpyHostToDevice);
+}
+
+int pfcg_upload_device(pfcg_handle* h, const double* d_fields) {
+	if (!h || !d_fields) return fail(h, PFCG_EARG, "NULL argument");
+	return h->prec == PFCG_FP64 ? do_upload<double>(h, d_fields, cudaMemcpyDeviceToDevice)
+	                            : do_upload<float>(h, d_fields, cudaMemcpyDeviceToDevice);
 }
 
 int pfcg_download(pfcg_handle* h, double* fields) {
 	if (!h || !fields) return fail(h, PFCG_EARG, "NULL argument");
-	return h->prec == PFCG_FP64 ? do_download<double>(h, fields) : do_download<float>(h, fields);
+	return h->prec == PFCG_FP64 ? do_download<double>(h, fields, cudaMemcpyDeviceToHost)
+	                            : do_download<float>(h, fields, cudaMemcpyDeviceToHost);
+}
+
+int pfcg_download_device(pfcg_handle* h, double* d_fields) {
+	if (!h || !d_fields) return fail(h, PFCG_EARG, "NULL argument");
+	return h->prec == PFCG_FP64 ? do_download<double>(h, d_fields, cudaMemcpyDeviceToDevice)
+	                            : do_download<float>(h, d_fields, cudaMemcpyDeviceToDevice);
+}
+
+int pfcg_warmstart(pfcg_handle* h, pfcg_fno* f) {
+	if (!h || !f) return fail(h, PFCG_EARG, "NULL argument");
+	if (h->U != 2) return fail(h, PFCG_EARG, "the warm-start network takes two fields");
+	return h->prec == PFCG_FP64 ? do_warmstart<double>(h, f) : do_warmstart<float>(h, f);
 }
 
 int pfcg_set_box(pfcg_handle* h, double dx, double dy) {

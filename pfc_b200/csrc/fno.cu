@@ -1,0 +1,865 @@
+// Fourier neural operator warm start: forward, backward, Adam and tiled apply.
+//
+// Network (fixed shape; two fields on a T x T periodic tile):
+//   v0 = P x + p                            lift, 2 -> C channels per pixel
+//   z_l = W_l v_l + b_l + K_l v_l,  v_{l+1} = gelu(z_l)  (l < L-1), v_L = z_{L-1}
+//   y = x + Q v_L + q                       projection C -> 2, added to the input
+// K_l v = irfft2 of R_l (complex C x C per retained mode) times rfft2(v) on the
+// retained modes kx in [0, MX), ky in {0..MY/2-1} u {T-MY/2..T-1}; all other
+// modes are dropped. The truncated transforms are direct sums against a
+// twiddle table (dft_x, dft_y, idft_x); the adjoint of each linear step is
+// another of these kernels, which is how the backward pass is built:
+//   idft_x^T = dft_x with the inverse's per-mode weights, dft_y^T = the
+//   inverse y sum, mix^T = mix with conj(R) transposed, dft_x^T = idft_x.
+// Activations and sums are FP32; the kernels read a BF16 copy of the FP32
+// master weights, which Adam updates.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/pfc_b200.h"
+#include "fno.cuh"
+
+namespace {
+
+constexpr int C = PFCG_FNO_CHANNELS;
+constexpr int L = PFCG_FNO_LAYERS;
+constexpr int MX = PFCG_FNO_MODES_X;
+constexpr int MY = PFCG_FNO_MODES_Y;
+constexpr int NK = MX * MY; // retained modes per channel pair
+
+// parameter layout, in floats: P [C][2], p [C], per layer {W [C][C], b [C],
+// Rr [C][C][NK], Ri [C][C][NK]} with R indexed [in][out][ky-row][kx], Q [2][C], q [2]
+constexpr size_t OFF_P = 0;
+constexpr size_t OFF_PB = OFF_P + C * 2;
+constexpr size_t OFF_L0 = OFF_PB + C;
+constexpr size_t LAYER = C * C + C + 2 * (size_t)C * C * NK;
+constexpr size_t OFF_Q = OFF_L0 + L * LAYER;
+constexpr size_t OFF_QB = OFF_Q + 2 * C;
+constexpr size_t NPARAM = OFF_QB + 2;
+static_assert(NPARAM == PFCG_FNO_PARAMS, "parameter count");
+
+__host__ __device__ constexpr size_t off_W(int l) { return OFF_L0 + l * LAYER; }
+__host__ __device__ constexpr size_t off_b(int l) { return off_W(l) + C * C; }
+__host__ __device__ constexpr size_t off_Rr(int l) { return off_b(l) + C; }
+__host__ __device__ constexpr size_t off_Ri(int l) { return off_Rr(l) + (size_t)C * C * NK; }
+
+constexpr int MAXT = 512; // largest tile (twiddle table in shared memory)
+
+__device__ __forceinline__ float wld(const __nv_bfloat16* w, size_t i) { return __bfloat162float(w[i]); }
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float z) {
+	return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * __expf(-0.5f * z * z);
+}
+
+// wave number of retained row k along y
+__device__ __forceinline__ int ky_of(int k, int T) { return k < MY / 2 ? k : T - MY + k; }
+
+__device__ __forceinline__ void load_tw(float2* sh, const float2* __restrict__ tw, int T) {
+	for (int i = threadIdx.x; i < T; i += blockDim.x) sh[i] = tw[i];
+	__syncthreads();
+}
+
+template <typename A> __device__ __forceinline__ A warp_sum(A a) {
+	for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+	return a;
+}
+
+// ------------------------------------------------------------- kernels ---
+
+// tw[j] = (cos, sin)(2 pi j / T), from FP64
+__global__ void twiddle_kernel(float2* tw, int T) {
+	for (int j = threadIdx.x + blockIdx.x * blockDim.x; j < T; j += blockDim.x * gridDim.x) {
+		double s, c;
+		sincospi(2.0 * j / (double)T, &s, &c);
+		tw[j] = make_float2((float)c, (float)s);
+	}
+}
+
+// v0[b][c][p] = P[c][0] x[b][0][p] + P[c][1] x[b][1][p] + p[c]
+__global__ void lift_fwd(const float* __restrict__ x, const __nv_bfloat16* __restrict__ w, float* __restrict__ v, int B,
+                         int npix) {
+	__shared__ float Ps[3 * C];
+	for (int i = threadIdx.x; i < 3 * C; i += blockDim.x) Ps[i] = wld(w, OFF_P + i);
+	__syncthreads();
+	const long long n = (long long)B * npix;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long b = t / npix;
+		const int p = (int)(t - b * npix);
+		const float x0 = x[(b * 2) * npix + p], x1 = x[(b * 2 + 1) * npix + p];
+		float* vb = v + b * C * npix + p;
+#pragma unroll 8
+		for (int c = 0; c < C; c++) vb[(long long)c * npix] = Ps[2 * c] * x0 + Ps[2 * c + 1] * x1 + Ps[2 * C + c];
+	}
+}
+
+// out[r][m] = scale[m] * sum_x in[r][x] exp(-2 pi i m x / T) for m < MX.
+// One warp per row: lanes stride over x, then a warp reduction per mode.
+__global__ void dft_x(const float* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
+                      const float* __restrict__ scale, long long nrows, int T) {
+	__shared__ float2 sh[MAXT];
+	load_tw(sh, tw, T);
+	const int lane = threadIdx.x & 31;
+	const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+	for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < nrows; r += warps) {
+		const float* row = in + r * T;
+		float ar[MX], ai[MX];
+#pragma unroll
+		for (int m = 0; m < MX; m++) ar[m] = ai[m] = 0.f;
+		for (int x = lane; x < T; x += 32) {
+			const float v = row[x];
+#pragma unroll
+			for (int m = 0; m < MX; m++) {
+				const float2 e = sh[(m * x) & (T - 1)];
+				ar[m] += v * e.x;
+				ai[m] -= v * e.y;
+			}
+		}
+		float xr = 0.f, xi = 0.f;
+#pragma unroll
+		for (int m = 0; m < MX; m++) {
+			const float sr = warp_sum(ar[m]), si = warp_sum(ai[m]);
+			if (lane == m) {
+				xr = sr;
+				xi = si;
+			}
+		}
+		if (lane < MX) {
+			const float sc = scale ? scale[lane] : 1.f;
+			out[r * MX + lane] = make_float2(xr * sc, xi * sc);
+		}
+	}
+}
+
+// out[r][x] (+)= sum_m scale[m] Re(in[r][m] exp(+2 pi i m x / T))
+__global__ void idft_x(const float2* __restrict__ in, float* __restrict__ out, const float2* __restrict__ tw,
+                       const float* __restrict__ scale, long long nrows, int T, int accumulate) {
+	__shared__ float2 sh[MAXT];
+	__shared__ float sc[MX];
+	if (threadIdx.x < MX) sc[threadIdx.x] = scale ? scale[threadIdx.x] : 1.f;
+	load_tw(sh, tw, T);
+	const long long n = nrows * T;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long r = t / T;
+		const int x = (int)(t - r * T);
+		const float2* row = in + r * MX;
+		float acc = 0.f;
+#pragma unroll
+		for (int m = 0; m < MX; m++) {
+			const float2 e = sh[(m * x) & (T - 1)];
+			const float2 z = row[m];
+			acc += sc[m] * (z.x * e.x - z.y * e.y);
+		}
+		out[t] = accumulate ? out[t] + acc : acc;
+	}
+}
+
+// Along y for each plane of [rows][MX] complex values:
+//   forward: out[k][m] = sum_y in[y][m] exp(-2 pi i ky(k) y / T), k < MY
+//   inverse: out[y][m] = sum_k in[k][m] exp(+2 pi i ky(k) y / T), y < T
+__global__ void dft_y(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
+                      long long nplanes, int T, int inverse) {
+	__shared__ float2 sh[MAXT];
+	load_tw(sh, tw, T);
+	const int nout = inverse ? T : MY;
+	const int nin = inverse ? MY : T;
+	for (long long plane = blockIdx.x; plane < nplanes; plane += gridDim.x) {
+		const float2* pin = in + plane * nin * MX;
+		float2* pout = out + plane * nout * MX;
+		for (int o = threadIdx.x; o < nout * MX; o += blockDim.x) {
+			const int q = o / MX, m = o - q * MX;
+			float ar = 0.f, ai = 0.f;
+			for (int j = 0; j < nin; j++) {
+				const int y = inverse ? q : j;
+				const int ky = ky_of(inverse ? j : q, T);
+				const float2 e = sh[(ky * y) & (T - 1)];
+				const float s = inverse ? e.y : -e.y;
+				const float2 z = pin[j * MX + m];
+				ar += z.x * e.x - z.y * s;
+				ai += z.x * s + z.y * e.x;
+			}
+			pout[o] = make_float2(ar, ai);
+		}
+	}
+}
+
+// mode mixing, per retained mode km:
+//   forward: out[b][o][km] = sum_i R[i][o][km] in[b][i][km]
+//   adjoint: out[b][i][km] = sum_o conj(R[i][o][km]) in[b][o][km]
+__global__ void mix(const float2* __restrict__ in, float2* __restrict__ out, const __nv_bfloat16* __restrict__ w, int l,
+                    int B, int adjoint) {
+	const long long n = (long long)B * C * NK;
+	const __nv_bfloat16* Rr = w + off_Rr(l);
+	const __nv_bfloat16* Ri = w + off_Ri(l);
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const int km = (int)(t % NK);
+		const int o = (int)((t / NK) % C);
+		const long long b = t / ((long long)NK * C);
+		const float2* ib = in + b * C * NK + km;
+		float ar = 0.f, ai = 0.f;
+#pragma unroll 8
+		for (int i = 0; i < C; i++) {
+			const size_t ri = adjoint ? ((size_t)o * C + i) * NK + km : ((size_t)i * C + o) * NK + km;
+			const float rr = __bfloat162float(Rr[ri]);
+			const float rm = adjoint ? -__bfloat162float(Ri[ri]) : __bfloat162float(Ri[ri]);
+			const float2 z = ib[(long long)i * NK];
+			ar += rr * z.x - rm * z.y;
+			ai += rr * z.y + rm * z.x;
+		}
+		out[t] = make_float2(ar, ai);
+	}
+}
+
+// dR[i][o][km] += sum_b dY[b][o][km] conj(X[b][i][km])
+__global__ void mix_grad(const float2* __restrict__ X, const float2* __restrict__ dY, float* __restrict__ g, int l, int B) {
+	const long long n = (long long)C * C * NK;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const int km = (int)(t % NK);
+		const int o = (int)((t / NK) % C);
+		const int i = (int)(t / ((long long)NK * C));
+		float gr = 0.f, gi = 0.f;
+		for (int b = 0; b < B; b++) {
+			const float2 x = X[((long long)b * C + i) * NK + km];
+			const float2 d = dY[((long long)b * C + o) * NK + km];
+			gr += d.x * x.x + d.y * x.y;
+			gi += d.y * x.x - d.x * x.y;
+		}
+		g[off_Rr(l) + t] += gr;
+		g[off_Ri(l) + t] += gi;
+	}
+}
+
+// z = W v + b + s; out = gelu(z) (act) or z. One thread per pixel.
+__global__ void __launch_bounds__(128) pointwise_fwd(const float* __restrict__ v, const float* __restrict__ s,
+                                                     const __nv_bfloat16* __restrict__ w, int l, float* __restrict__ z,
+                                                     float* __restrict__ out, int B, int npix, int act) {
+	__shared__ float Ws[C][C];
+	__shared__ float bs[C];
+	for (int i = threadIdx.x; i < C * C; i += blockDim.x) Ws[i / C][i % C] = wld(w, off_W(l) + i);
+	for (int i = threadIdx.x; i < C; i += blockDim.x) bs[i] = wld(w, off_b(l) + i);
+	__syncthreads();
+	const long long n = (long long)B * npix;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long b = t / npix;
+		const long long base = b * C * npix + (t - b * npix);
+		float in[C];
+#pragma unroll
+		for (int i = 0; i < C; i++) in[i] = v[base + (long long)i * npix];
+#pragma unroll 4
+		for (int o = 0; o < C; o++) {
+			float acc = bs[o] + s[base + (long long)o * npix];
+#pragma unroll
+			for (int i = 0; i < C; i++) acc += Ws[o][i] * in[i];
+			if (z) z[base + (long long)o * npix] = acc;
+			out[base + (long long)o * npix] = act ? gelu(acc) : acc;
+		}
+	}
+}
+
+// dz = dout * g'(z) (also the gradient of the spectral branch); dv = W^T dz
+__global__ void __launch_bounds__(128) pointwise_bwd(const float* __restrict__ z, const float* __restrict__ dout,
+                                                     const __nv_bfloat16* __restrict__ w, int l, float* __restrict__ dz,
+                                                     float* __restrict__ dv, int B, int npix, int act) {
+	__shared__ float Ws[C][C];
+	for (int i = threadIdx.x; i < C * C; i += blockDim.x) Ws[i / C][i % C] = wld(w, off_W(l) + i);
+	__syncthreads();
+	const long long n = (long long)B * npix;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long b = t / npix;
+		const long long base = b * C * npix + (t - b * npix);
+		float d[C];
+#pragma unroll
+		for (int o = 0; o < C; o++) {
+			const float g = dout[base + (long long)o * npix];
+			d[o] = act ? g * gelu_d(z[base + (long long)o * npix]) : g;
+			dz[base + (long long)o * npix] = d[o];
+		}
+#pragma unroll 4
+		for (int i = 0; i < C; i++) {
+			float acc = 0.f;
+#pragma unroll
+			for (int o = 0; o < C; o++) acc += Ws[o][i] * d[o];
+			dv[base + (long long)i * npix] = acc;
+		}
+	}
+}
+
+// dW[o][i] += sum_p dz[o][p] v[i][p], db[o] += sum_p dz[o][p]: a C x C product
+// over all pixels. Each block stages 64-pixel tiles of dz and v in shared
+// memory; thread t owns W entries (o = t / 8, i = 4 (t % 8) .. +3).
+constexpr int WG_TILE = 64;
+__global__ void __launch_bounds__(256) weight_grad(const float* __restrict__ dz, const float* __restrict__ v,
+                                                   float* __restrict__ gW, float* __restrict__ gb, int B, int npix) {
+	__shared__ float sd[C][WG_TILE + 1];
+	__shared__ float sv[C][WG_TILE + 1];
+	const int o = threadIdx.x >> 3, i0 = (threadIdx.x & 7) * 4;
+	float acc[4] = {0.f, 0.f, 0.f, 0.f}, accb = 0.f;
+	const int tiles_per_image = npix / WG_TILE;
+	const long long ntiles = (long long)B * tiles_per_image;
+	for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+		const long long b = tile / tiles_per_image;
+		const int p0 = (int)(tile - b * tiles_per_image) * WG_TILE;
+		__syncthreads();
+		for (int e = threadIdx.x; e < C * WG_TILE; e += blockDim.x) {
+			const int c = e / WG_TILE, p = e % WG_TILE;
+			const long long gi = (b * C + c) * (long long)npix + p0 + p;
+			sd[c][p] = dz[gi];
+			sv[c][p] = v[gi];
+		}
+		__syncthreads();
+#pragma unroll 8
+		for (int p = 0; p < WG_TILE; p++) {
+			const float d = sd[o][p];
+#pragma unroll
+			for (int k = 0; k < 4; k++) acc[k] += d * sv[i0 + k][p];
+			accb += d;
+		}
+	}
+#pragma unroll
+	for (int k = 0; k < 4; k++) atomicAdd(&gW[o * C + i0 + k], acc[k]);
+	if ((threadIdx.x & 7) == 0) atomicAdd(&gb[o], accb);
+}
+
+// y = x + Q v + q; with a target also loss += sum (y - t)^2 / n and dy = 2 (y - t) / n
+__global__ void proj_fwd_loss(const float* __restrict__ x, const float* __restrict__ v, const __nv_bfloat16* __restrict__ w,
+                              float* __restrict__ y, const float* __restrict__ target, float* __restrict__ dy,
+                              double* __restrict__ loss, int B, int npix) {
+	__shared__ float Qs[2 * C + 2];
+	__shared__ double red[32];
+	for (int i = threadIdx.x; i < 2 * C + 2; i += blockDim.x) Qs[i] = wld(w, OFF_Q + i);
+	__syncthreads();
+	const long long n = (long long)B * npix;
+	const float inv = 2.f / (float)(2 * n);
+	double acc = 0.0;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long b = t / npix;
+		const int p = (int)(t - b * npix);
+		const float* vb = v + b * C * npix + p;
+		float o0 = Qs[2 * C], o1 = Qs[2 * C + 1];
+#pragma unroll 8
+		for (int c = 0; c < C; c++) {
+			const float vv = vb[(long long)c * npix];
+			o0 += Qs[c] * vv;
+			o1 += Qs[C + c] * vv;
+		}
+		const long long i0 = b * 2 * npix + p, i1 = i0 + npix;
+		const float y0 = x[i0] + o0, y1 = x[i1] + o1;
+		y[i0] = y0;
+		y[i1] = y1;
+		if (target) {
+			const float e0 = y0 - target[i0], e1 = y1 - target[i1];
+			acc += (double)e0 * e0 + (double)e1 * e1;
+			dy[i0] = inv * e0;
+			dy[i1] = inv * e1;
+		}
+	}
+	if (target) {
+		acc = warp_sum(acc);
+		if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+		__syncthreads();
+		if (threadIdx.x < 32) {
+			double a = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+			a = warp_sum(a);
+			if (threadIdx.x == 0) atomicAdd(loss, a / (double)(2 * n));
+		}
+	}
+}
+
+// dv = Q^T dy
+__global__ void proj_bwd(const float* __restrict__ dy, const __nv_bfloat16* __restrict__ w, float* __restrict__ dv, int B,
+                         int npix) {
+	__shared__ float Qs[2 * C];
+	for (int i = threadIdx.x; i < 2 * C; i += blockDim.x) Qs[i] = wld(w, OFF_Q + i);
+	__syncthreads();
+	const long long n = (long long)B * npix;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long b = t / npix;
+		const int p = (int)(t - b * npix);
+		const float d0 = dy[b * 2 * npix + p], d1 = dy[b * 2 * npix + npix + p];
+		float* db = dv + b * C * npix + p;
+#pragma unroll 8
+		for (int c = 0; c < C; c++) db[(long long)c * npix] = Qs[c] * d0 + Qs[C + c] * d1;
+	}
+}
+
+// Per-channel sums over all pixels of a[b][c][p] * e[b][j][p] (j = 0, 1; e a
+// two-field tensor) and of a itself. Gradients of the lift (a = dv0, e = x;
+// g_ae = dP [C][2], g_a = dp [C]) and of the projection (a = v_L, e = dy;
+// g_ae = dQ [2][C]). One block row per channel (blockIdx.y).
+__global__ void channel_grad(const float* __restrict__ a, const float* __restrict__ e, float* __restrict__ g_ae,
+                             int stride_c, int stride_j, float* __restrict__ g_a, int B, int npix) {
+	__shared__ float red[3][32];
+	const int c = blockIdx.y;
+	const long long n = (long long)B * npix;
+	float s0 = 0.f, s1 = 0.f, sa = 0.f;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long b = t / npix;
+		const int p = (int)(t - b * npix);
+		const float av = a[(b * C + c) * npix + p];
+		s0 += av * e[(b * 2) * npix + p];
+		s1 += av * e[(b * 2 + 1) * npix + p];
+		sa += av;
+	}
+	s0 = warp_sum(s0);
+	s1 = warp_sum(s1);
+	sa = warp_sum(sa);
+	if ((threadIdx.x & 31) == 0) {
+		red[0][threadIdx.x >> 5] = s0;
+		red[1][threadIdx.x >> 5] = s1;
+		red[2][threadIdx.x >> 5] = sa;
+	}
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		const bool in = threadIdx.x < (blockDim.x >> 5);
+		s0 = warp_sum(in ? red[0][threadIdx.x] : 0.f);
+		s1 = warp_sum(in ? red[1][threadIdx.x] : 0.f);
+		sa = warp_sum(in ? red[2][threadIdx.x] : 0.f);
+		if (threadIdx.x == 0) {
+			atomicAdd(&g_ae[c * stride_c], s0);
+			atomicAdd(&g_ae[c * stride_c + stride_j], s1);
+			if (g_a) atomicAdd(&g_a[c], sa);
+		}
+	}
+}
+
+// g[j] += sum over pixels of e[b][j][p], j = 0, 1
+__global__ void sum2_kernel(const float* __restrict__ e, float* __restrict__ g, int B, int npix) {
+	const long long n = (long long)B * npix;
+	float s0 = 0.f, s1 = 0.f;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const long long b = t / npix;
+		const int p = (int)(t - b * npix);
+		s0 += e[b * 2 * npix + p];
+		s1 += e[b * 2 * npix + npix + p];
+	}
+	s0 = warp_sum(s0);
+	s1 = warp_sum(s1);
+	if ((threadIdx.x & 31) == 0) {
+		atomicAdd(&g[0], s0);
+		atomicAdd(&g[1], s1);
+	}
+}
+
+__global__ void to_bf16(const float* __restrict__ a, __nv_bfloat16* __restrict__ b, long long n) {
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		b[i] = __float2bfloat16(a[i]);
+}
+
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+		const float gi = g[i];
+		const float mi = b1 * m[i] + (1.f - b1) * gi;
+		const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+		m[i] = mi;
+		v[i] = vi;
+		p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+	}
+}
+
+// Tiles of a periodic two-field FP64 grid as FP32 network input. Tile j of the
+// batch is block (first + j) of the grid's core x core blocks (row-major over
+// tiles_x columns) plus halo points on each side, wrapped periodically.
+__global__ void gather_tiles(const double* __restrict__ f, float* __restrict__ out, int Nx, int Ny, int T, int core,
+                             int halo, int tiles_x, int first, int count) {
+	const long long per = 2LL * T * T;
+	const long long n = per * count;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const int j = (int)(t / per);
+		const int r = (int)(t - (long long)j * per);
+		const int u = r / (T * T), q = r - u * T * T;
+		const int ty = q / T, tx = q - ty * T;
+		const int tile = first + j;
+		const int by = tile / tiles_x, bx = tile - by * tiles_x;
+		int x = (bx * core - halo + tx) % Nx, y = (by * core - halo + ty) % Ny;
+		if (x < 0) x += Nx;
+		if (y < 0) y += Ny;
+		out[t] = (float)f[((long long)u * Ny + y) * Nx + x];
+	}
+}
+
+// Writes each tile's core block of the network output back to the grid.
+__global__ void scatter_tiles(const float* __restrict__ in, double* __restrict__ f, int Nx, int Ny, int T, int core,
+                              int halo, int tiles_x, int first, int count) {
+	const long long per = 2LL * core * core;
+	const long long n = per * count;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const int j = (int)(t / per);
+		const int r = (int)(t - (long long)j * per);
+		const int u = r / (core * core), q = r - u * core * core;
+		const int cy = q / core, cx = q - cy * core;
+		const int tile = first + j;
+		const int by = tile / tiles_x, bx = tile - by * tiles_x;
+		const int x = bx * core + cx, y = by * core + cy;
+		if (x >= Nx || y >= Ny) continue;
+		f[((long long)u * Ny + y) * Nx + x] =
+		    (double)in[(long long)j * 2 * T * T + ((long long)u * T + halo + cy) * T + halo + cx];
+	}
+}
+
+// Per-block FP64 partial sums of (out - in) for each of the two fields.
+constexpr int MEAN_BLOCKS = 296;
+__global__ void diff_partials(const double* __restrict__ in, const double* __restrict__ out, double* __restrict__ part,
+                              long long npts) {
+	__shared__ double red[2][32];
+	for (int u = 0; u < 2; u++) {
+		double s = 0.0;
+		for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npts;
+		     i += (long long)gridDim.x * blockDim.x)
+			s += out[u * npts + i] - in[u * npts + i];
+		s = warp_sum(s);
+		if ((threadIdx.x & 31) == 0) red[u][threadIdx.x >> 5] = s;
+	}
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		for (int u = 0; u < 2; u++) {
+			double s = threadIdx.x < (blockDim.x >> 5) ? red[u][threadIdx.x] : 0.0;
+			s = warp_sum(s);
+			if (threadIdx.x == 0) part[u * gridDim.x + blockIdx.x] = s;
+		}
+	}
+}
+
+// out[u] -= (sum of the partials of u) / npts: gives each field back the
+// input's mean (the relaxation conserves it). Fixed summation order.
+__global__ void restore_means(double* __restrict__ out, const double* __restrict__ part, int nparts, long long npts) {
+	__shared__ double shift[2];
+	if (threadIdx.x < 2) {
+		double s = 0.0;
+		for (int i = 0; i < nparts; i++) s += part[threadIdx.x * nparts + i];
+		shift[threadIdx.x] = s / (double)npts;
+	}
+	__syncthreads();
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * npts;
+	     i += (long long)gridDim.x * blockDim.x)
+		out[i] -= shift[i >= npts];
+}
+
+int grid_for(long long n, int block) {
+	long long g = (n + block - 1) / block;
+	return (int)(g > 148 * 16 ? 148 * 16 : (g < 1 ? 1 : g));
+}
+
+int planes_grid(long long nplanes) { return (int)std::min<long long>(nplanes, 148 * 8); }
+
+thread_local std::string g_fno_err;
+
+} // namespace
+
+struct pfcg_fno {
+	int T = 0, maxB = 0;
+	cudaStream_t stream = nullptr;
+	float* p = nullptr;          // master weights (FP32)
+	__nv_bfloat16* w = nullptr;  // BF16 copy read by the kernels
+	float* g = nullptr;          // gradients
+	float* am = nullptr;         // Adam moments
+	float* av = nullptr;
+	long long adam_t = 0;
+	float2* tw = nullptr;        // twiddles of the tile size
+	float* sx = nullptr;         // per-kx weights of the truncated irfft2: (kx ? 2 : 1) / T^2
+	float* v[L + 1] = {};        // layer inputs (v[L] feeds the projection)
+	float* z[L] = {};            // pre-activations
+	float* s = nullptr;          // spectral branch output
+	float2* A = nullptr;         // [B][C][T][MX] x-transformed rows (and adjoint scratch)
+	float2* X[L] = {};           // [B][C][MY][MX] retained modes of each layer input
+	float2* Y = nullptr;         // [B][C][MY][MX] mixed modes
+	float2* Bq = nullptr;        // [B][C][T][MX] y-inverse rows (and adjoint scratch)
+	float* dv = nullptr;         // gradient scratch
+	float* dv2 = nullptr;
+	float* dz = nullptr;
+	float* x = nullptr;          // [B][2][T][T] tile input (apply)
+	float* y = nullptr;          // [B][2][T][T] network output
+	float* dy = nullptr;
+	double* loss = nullptr;
+	double* field_tmp = nullptr; // grid-sized scratch for the warm start
+	size_t field_tmp_n = 0;
+	double* part = nullptr;      // mean partial sums [2][MEAN_BLOCKS]
+	long long launches = 0;
+	std::string err;
+};
+
+namespace {
+
+int ffail(pfcg_fno* f, int code, const std::string& m) {
+	if (f) f->err = m;
+	g_fno_err = m;
+	return code;
+}
+
+#define FCK(call)                                                                                                      \
+	do {                                                                                                           \
+		cudaError_t e_ = (call);                                                                               \
+		if (e_ != cudaSuccess) return ffail(f, PFCG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+	} while (0)
+
+// forward pass over a batch of B tiles; with train the pre-activations are kept for backward
+int forward(pfcg_fno* f, const float* x, int B, const float* target, bool train) {
+	const int T = f->T, npix = T * T;
+	const long long rows = (long long)B * C * T, planes = (long long)B * C;
+	cudaStream_t st = f->stream;
+	lift_fwd<<<grid_for((long long)B * npix, 256), 256, 0, st>>>(x, f->w, f->v[0], B, npix);
+	f->launches++;
+	for (int l = 0; l < L; l++) {
+		dft_x<<<grid_for(rows * 32, 256), 256, 0, st>>>(f->v[l], f->A, f->tw, nullptr, rows, T);
+		dft_y<<<planes_grid(planes), 128, 0, st>>>(f->A, f->X[l], f->tw, planes, T, 0);
+		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->w, l, B, 0);
+		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Y, f->Bq, f->tw, planes, T, 1);
+		idft_x<<<grid_for(rows * T, 256), 256, 0, st>>>(f->Bq, f->s, f->tw, f->sx, rows, T, 0);
+		pointwise_fwd<<<grid_for((long long)B * npix, 128), 128, 0, st>>>(f->v[l], f->s, f->w, l, train ? f->z[l] : nullptr,
+		                                                                    f->v[l + 1], B, npix, l < L - 1);
+		f->launches += 6;
+	}
+	if (target) FCK(cudaMemsetAsync(f->loss, 0, sizeof(double), st));
+	proj_fwd_loss<<<grid_for((long long)B * npix, 256), 256, 0, st>>>(x, f->v[L], f->w, f->y, target, f->dy, f->loss, B,
+	                                                                 npix);
+	f->launches++;
+	FCK(cudaGetLastError());
+	return 0;
+}
+
+int backward(pfcg_fno* f, const float* x, int B) {
+	const int T = f->T, npix = T * T;
+	const long long rows = (long long)B * C * T, planes = (long long)B * C;
+	cudaStream_t st = f->stream;
+	const dim3 cg(std::min(grid_for((long long)B * npix, 256), 64), C);
+	const int wg = std::min(grid_for((long long)B * npix / WG_TILE, 1), 148 * 4);
+	FCK(cudaMemsetAsync(f->g, 0, sizeof(float) * NPARAM, st));
+	// projection: dQ[j][c] = sum v_L[c] dy[j], dq[j] = sum dy[j], dv_L = Q^T dy
+	channel_grad<<<cg, 256, 0, st>>>(f->v[L], f->dy, f->g + OFF_Q, 1, C, nullptr, B, npix);
+	sum2_kernel<<<grid_for((long long)B * npix, 256), 256, 0, st>>>(f->dy, f->g + OFF_QB, B, npix);
+	proj_bwd<<<grid_for((long long)B * npix, 256), 256, 0, st>>>(f->dy, f->w, f->dv, B, npix);
+	f->launches += 3;
+	for (int l = L - 1; l >= 0; l--) {
+		pointwise_bwd<<<grid_for((long long)B * npix, 128), 128, 0, st>>>(f->z[l], f->dv, f->w, l, f->dz, f->dv2, B, npix,
+		                                                                    l < L - 1);
+		weight_grad<<<wg, 256, 0, st>>>(f->dz, f->v[l], f->g + off_W(l), f->g + off_b(l), B, npix);
+		// spectral branch, in reverse
+		dft_x<<<grid_for(rows * 32, 256), 256, 0, st>>>(f->dz, f->Bq, f->tw, f->sx, rows, T);
+		dft_y<<<planes_grid(planes), 128, 0, st>>>(f->Bq, f->Y, f->tw, planes, T, 0);
+		mix_grad<<<grid_for((long long)C * C * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->g, l, B);
+		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->Y, f->Bq, f->w, l, B, 1);
+		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Bq, f->A, f->tw, planes, T, 1);
+		idft_x<<<grid_for(rows * T, 256), 256, 0, st>>>(f->A, f->dv2, f->tw, nullptr, rows, T, 1);
+		f->launches += 8;
+		std::swap(f->dv, f->dv2);
+	}
+	// lift: dP[c][j] = sum dv0[c] x[j], dp[c] = sum dv0[c]
+	channel_grad<<<cg, 256, 0, st>>>(f->dv, x, f->g + OFF_P, 2, 1, f->g + OFF_PB, B, npix);
+	f->launches++;
+	FCK(cudaGetLastError());
+	return 0;
+}
+
+} // namespace
+
+int fno_apply_device(pfcg_fno* f, const double* d_in, double* d_out, int Nx, int Ny, cudaStream_t st) {
+	const int T = f->T, halo = T / 4, core = T - 2 * halo;
+	const int tx = (Nx + core - 1) / core, ty = (Ny + core - 1) / core;
+	const int ntiles = tx * ty;
+	const cudaStream_t own = f->stream;
+	cudaEvent_t ev;
+	FCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+	FCK(cudaEventRecord(ev, st));
+	FCK(cudaStreamWaitEvent(own, ev, 0));
+	for (int first = 0; first < ntiles; first += f->maxB) {
+		const int count = std::min(f->maxB, ntiles - first);
+		gather_tiles<<<grid_for(2LL * T * T * count, 256), 256, 0, own>>>(d_in, f->x, Nx, Ny, T, core, halo, tx, first,
+		                                                                  count);
+		f->launches++;
+		int rc = forward(f, f->x, count, nullptr, false);
+		if (rc) return rc;
+		scatter_tiles<<<grid_for(2LL * core * core * count, 256), 256, 0, own>>>(f->y, d_out, Nx, Ny, T, core, halo, tx,
+		                                                                         first, count);
+		f->launches++;
+	}
+	const long long npts = (long long)Nx * Ny;
+	diff_partials<<<MEAN_BLOCKS, 256, 0, own>>>(d_in, d_out, f->part, npts);
+	restore_means<<<grid_for(2 * npts, 256), 256, 0, own>>>(d_out, f->part, MEAN_BLOCKS, npts);
+	f->launches += 2;
+	FCK(cudaGetLastError());
+	FCK(cudaEventRecord(ev, own));
+	FCK(cudaStreamWaitEvent(st, ev, 0));
+	FCK(cudaEventDestroy(ev));
+	return 0;
+}
+
+int fno_scratch_grid(pfcg_fno* f, size_t n, double** out) {
+	if (f->field_tmp_n < n) {
+		cudaFree(f->field_tmp);
+		f->field_tmp = nullptr;
+		f->field_tmp_n = 0;
+		FCK(cudaMalloc(&f->field_tmp, sizeof(double) * n));
+		f->field_tmp_n = n;
+	}
+	*out = f->field_tmp;
+	return 0;
+}
+
+const char* fno_error(const pfcg_fno* f) { return f->err.c_str(); }
+
+extern "C" {
+
+size_t pfcg_fno_param_count(void) { return NPARAM; }
+
+int pfcg_fno_create(int tile, int max_batch, pfcg_fno** out) {
+	if (!out) return ffail(nullptr, PFCG_EARG, "NULL argument");
+	*out = nullptr;
+	if (tile < 2 * MY || tile > MAXT || (tile & (tile - 1)) != 0 || max_batch < 1)
+		return ffail(nullptr, PFCG_EARG, "tile must be a power of two in [32, 512] and max_batch >= 1");
+	pfcg_fno* f = new pfcg_fno();
+	f->T = tile;
+	f->maxB = max_batch;
+	const long long npix = (long long)tile * tile;
+	const size_t nv = (size_t)max_batch * C * npix;
+	cudaError_t e = cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking);
+	std::vector<void**> bufs;
+	std::vector<size_t> sizes;
+	auto add = [&](void** ptr, size_t bytes) {
+		bufs.push_back(ptr);
+		sizes.push_back(bytes);
+	};
+	// the first five (weights, gradients, moments) are cleared below
+	add((void**)&f->p, sizeof(float) * NPARAM);
+	add((void**)&f->w, sizeof(__nv_bfloat16) * NPARAM);
+	add((void**)&f->g, sizeof(float) * NPARAM);
+	add((void**)&f->am, sizeof(float) * NPARAM);
+	add((void**)&f->av, sizeof(float) * NPARAM);
+	add((void**)&f->tw, sizeof(float2) * tile);
+	add((void**)&f->sx, sizeof(float) * MX);
+	for (int l = 0; l <= L; l++) add((void**)&f->v[l], sizeof(float) * nv);
+	for (int l = 0; l < L; l++) add((void**)&f->z[l], sizeof(float) * nv);
+	for (int l = 0; l < L; l++) add((void**)&f->X[l], sizeof(float2) * max_batch * C * NK);
+	add((void**)&f->s, sizeof(float) * nv);
+	add((void**)&f->A, sizeof(float2) * max_batch * C * tile * MX);
+	add((void**)&f->Y, sizeof(float2) * max_batch * C * NK);
+	add((void**)&f->Bq, sizeof(float2) * max_batch * C * tile * MX);
+	add((void**)&f->dv, sizeof(float) * nv);
+	add((void**)&f->dv2, sizeof(float) * nv);
+	add((void**)&f->dz, sizeof(float) * nv);
+	add((void**)&f->x, sizeof(float) * max_batch * 2 * npix);
+	add((void**)&f->y, sizeof(float) * max_batch * 2 * npix);
+	add((void**)&f->dy, sizeof(float) * max_batch * 2 * npix);
+	add((void**)&f->loss, sizeof(double));
+	add((void**)&f->part, sizeof(double) * 2 * MEAN_BLOCKS);
+	for (size_t i = 0; i < bufs.size() && e == cudaSuccess; i++) e = cudaMalloc(bufs[i], sizes[i]);
+	if (e != cudaSuccess) {
+		pfcg_fno_destroy(f);
+		return ffail(nullptr, PFCG_ENOMEM, std::string("device allocation: ") + cudaGetErrorString(e));
+	}
+	float sc[MX];
+	for (int m = 0; m < MX; m++) sc[m] = (m == 0 ? 1.f : 2.f) / (float)npix;
+	e = cudaMemcpyAsync(f->sx, sc, sizeof(sc), cudaMemcpyHostToDevice, f->stream);
+	twiddle_kernel<<<1, 256, 0, f->stream>>>(f->tw, tile);
+	f->launches++;
+	for (size_t i = 0; i < 5 && e == cudaSuccess; i++) e = cudaMemsetAsync(*bufs[i], 0, sizes[i], f->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
+	if (e == cudaSuccess) e = cudaGetLastError();
+	if (e != cudaSuccess) {
+		pfcg_fno_destroy(f);
+		return ffail(nullptr, PFCG_ECUDA, std::string("set-up: ") + cudaGetErrorString(e));
+	}
+	*out = f;
+	return 0;
+}
+
+void pfcg_fno_destroy(pfcg_fno* f) {
+	if (!f) return;
+	if (f->stream) cudaStreamSynchronize(f->stream);
+	void* ptrs[] = {f->p,  f->w,  f->g,   f->am, f->av, f->tw, f->sx,   f->s,         f->A,   f->Y,
+	                f->Bq, f->dv, f->dv2, f->dz, f->x,  f->y,  f->dy, f->loss, f->field_tmp, f->part};
+	for (void* q : ptrs) cudaFree(q);
+	for (int l = 0; l <= L; l++) cudaFree(f->v[l]);
+	for (int l = 0; l < L; l++) {
+		cudaFree(f->z[l]);
+		cudaFree(f->X[l]);
+	}
+	if (f->stream) cudaStreamDestroy(f->stream);
+	delete f;
+}
+
+int pfcg_fno_set_params(pfcg_fno* f, const float* host_params) {
+	if (!f || !host_params) return ffail(f, PFCG_EARG, "NULL argument");
+	FCK(cudaMemcpyAsync(f->p, host_params, sizeof(float) * NPARAM, cudaMemcpyHostToDevice, f->stream));
+	to_bf16<<<grid_for(NPARAM, 256), 256, 0, f->stream>>>(f->p, f->w, NPARAM);
+	f->launches++;
+	FCK(cudaMemsetAsync(f->am, 0, sizeof(float) * NPARAM, f->stream));
+	FCK(cudaMemsetAsync(f->av, 0, sizeof(float) * NPARAM, f->stream));
+	f->adam_t = 0;
+	FCK(cudaStreamSynchronize(f->stream));
+	return 0;
+}
+
+int pfcg_fno_get_params(pfcg_fno* f, float* host_params) {
+	if (!f || !host_params) return ffail(f, PFCG_EARG, "NULL argument");
+	FCK(cudaMemcpyAsync(host_params, f->p, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost, f->stream));
+	FCK(cudaStreamSynchronize(f->stream));
+	return 0;
+}
+
+int pfcg_fno_forward(pfcg_fno* f, const float* d_in, float* d_out, int batch) {
+	if (!f || !d_in || !d_out) return ffail(f, PFCG_EARG, "NULL argument");
+	if (batch < 1 || batch > f->maxB) return ffail(f, PFCG_EARG, "batch outside [1, max_batch]");
+	int rc = forward(f, d_in, batch, nullptr, false);
+	if (rc) return rc;
+	FCK(cudaMemcpyAsync(d_out, f->y, sizeof(float) * batch * 2 * f->T * f->T, cudaMemcpyDeviceToDevice, f->stream));
+	FCK(cudaStreamSynchronize(f->stream));
+	return 0;
+}
+
+int pfcg_fno_loss_grad(pfcg_fno* f, const float* d_in, const float* d_target, int batch, double* loss,
+                       float* host_grad) {
+	if (!f || !d_in || !d_target) return ffail(f, PFCG_EARG, "NULL argument");
+	if (batch < 1 || batch > f->maxB) return ffail(f, PFCG_EARG, "batch outside [1, max_batch]");
+	int rc = forward(f, d_in, batch, d_target, true);
+	if (!rc) rc = backward(f, d_in, batch);
+	if (rc) return rc;
+	if (loss) FCK(cudaMemcpyAsync(loss, f->loss, sizeof(double), cudaMemcpyDeviceToHost, f->stream));
+	if (host_grad) FCK(cudaMemcpyAsync(host_grad, f->g, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost, f->stream));
+	FCK(cudaStreamSynchronize(f->stream));
+	return 0;
+}
+
+int pfcg_fno_adam_step(pfcg_fno* f, float lr, float beta1, float beta2, float eps) {
+	if (!f) return ffail(f, PFCG_EARG, "NULL argument");
+	f->adam_t++;
+	const float c1 = 1.f - std::pow(beta1, (float)f->adam_t), c2 = 1.f - std::pow(beta2, (float)f->adam_t);
+	adam_kernel<<<grid_for(NPARAM, 256), 256, 0, f->stream>>>(f->p, f->g, f->am, f->av, NPARAM, lr, beta1, beta2, eps,
+	                                                           c1, c2);
+	to_bf16<<<grid_for(NPARAM, 256), 256, 0, f->stream>>>(f->p, f->w, NPARAM);
+	f->launches += 2;
+	FCK(cudaGetLastError());
+	return 0;
+}
+
+int pfcg_fno_apply(pfcg_fno* f, const double* d_in, double* d_out, int Nx, int Ny, void* stream) {
+	if (!f || !d_in || !d_out) return ffail(f, PFCG_EARG, "NULL argument");
+	if (d_in == d_out) return ffail(f, PFCG_EARG, "input and output grids must be distinct");
+	if (Nx < 1 || Ny < 1) return ffail(f, PFCG_EARG, "empty grid");
+	cudaStream_t st = (cudaStream_t)stream;
+	int rc = fno_apply_device(f, d_in, d_out, Nx, Ny, st);
+	if (rc) return rc;
+	FCK(cudaStreamSynchronize(st));
+	return 0;
+}
+
+int pfcg_fno_stream(const pfcg_fno* f, void** stream) {
+	if (!f || !stream) return PFCG_EARG;
+	*stream = (void*)f->stream;
+	return 0;
+}
+
+int pfcg_fno_launch_count(const pfcg_fno* f, long long* count) {
+	if (!f || !count) return PFCG_EARG;
+	*count = f->launches;
+	return 0;
+}
+
+const char* pfcg_fno_last_error(const pfcg_fno* f) { return f ? f->err.c_str() : g_fno_err.c_str(); }
+
+} // extern "C"

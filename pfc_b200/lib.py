@@ -34,6 +34,10 @@ SIGNATURES = {
                                    ctypes.POINTER(ctypes.c_void_p)]),
     "pfcg_upload": (ctypes.c_int, [_vp, _dp]),
     "pfcg_download": (ctypes.c_int, [_vp, _dp]),
+    "pfcg_upload_device": (ctypes.c_int, [_vp, _vp]),
+    "pfcg_download_device": (ctypes.c_int, [_vp, _vp]),
+    "pfcg_init_hetero": (ctypes.c_int, [_vp, _ip, _ip, ctypes.c_double, ctypes.c_double, _vp, _vp]),
+    "pfcg_init_last_error": (ctypes.c_char_p, []),
     "pfcg_set_box": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     "pfcg_get_box": (ctypes.c_int, [_vp, _dp, _dp]),
     "pfcg_set_time": (ctypes.c_int, [_vp, _ip]),
@@ -55,6 +59,19 @@ SIGNATURES = {
     "pfcg_batch_launches": (ctypes.c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_longlong),
                                            ctypes.POINTER(ctypes.c_longlong)]),
     "pfcg_batch_destroy": (None, [_vp]),
+    "pfcg_fno_param_count": (ctypes.c_size_t, []),
+    "pfcg_fno_create": (ctypes.c_int, [_ip, _ip, ctypes.POINTER(ctypes.c_void_p)]),
+    "pfcg_fno_set_params": (ctypes.c_int, [_vp, _vp]),
+    "pfcg_fno_get_params": (ctypes.c_int, [_vp, _vp]),
+    "pfcg_fno_forward": (ctypes.c_int, [_vp, _vp, _vp, _ip]),
+    "pfcg_fno_loss_grad": (ctypes.c_int, [_vp, _vp, _vp, _ip, _dp, _vp]),
+    "pfcg_fno_adam_step": (ctypes.c_int, [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
+    "pfcg_fno_apply": (ctypes.c_int, [_vp, _vp, _vp, _ip, _ip, _vp]),
+    "pfcg_warmstart": (ctypes.c_int, [_vp, _vp]),
+    "pfcg_fno_stream": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
+    "pfcg_fno_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "pfcg_fno_last_error": (ctypes.c_char_p, [_vp]),
+    "pfcg_fno_destroy": (None, [_vp]),
     "pfcg_stream": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
     "pfcg_launch_count": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "pfcg_last_error": (ctypes.c_char_p, [_vp]),
@@ -149,6 +166,18 @@ class Relaxation:
         self._check(self.L.pfcg_download(self.h, _dptr(out)))
         return out
 
+    def upload_device(self, ptr: int) -> None:
+        """Uploads U*Ny*Nx doubles from DEVICE memory at ptr."""
+        self._check(self.L.pfcg_upload_device(self.h, ctypes.c_void_p(ptr)))
+
+    def download_device(self, ptr: int) -> None:
+        """Downloads the fields to U*Ny*Nx doubles of DEVICE memory at ptr."""
+        self._check(self.L.pfcg_download_device(self.h, ctypes.c_void_p(ptr)))
+
+    def warmstart(self, net) -> None:
+        """Replaces the fields by the warm-start network's proposal (U = 2)."""
+        self._check(self.L.pfcg_warmstart(self.h, net.f))
+
     def step(self, n: int = 1) -> int:
         """Advances n steps; returns 0, or raises PfcError (code 39 for NaN)."""
         rc = self.L.pfcg_step(self.h, n)
@@ -240,6 +269,23 @@ class Relaxation:
             t = nxt
         return np.array(rows)
 
+    def relax_until(self, tol: float = 1e-9, every: int = 100, max_steps: int = 100000):
+        """Steps until the free energy changes by less than tol per step, measured
+        as |<f>(t) - <f>(t - every)| / every at every `every` steps. Returns
+        (steps taken, final <f>, seconds); steps is None if max_steps ran out."""
+        import time
+        t0 = time.perf_counter()
+        prev = self.evaluate()[0]
+        done = 0
+        while done < max_steps:
+            self.step(every)
+            done += every
+            f = self.evaluate()[0]
+            if abs(f - prev) / every < tol:
+                return done, f, time.perf_counter() - t0
+            prev = f
+        return None, prev, time.perf_counter() - t0
+
 
 def relax_noalloc(params: Params, Nx: int, Ny: int, dx: float, dy: float, nsteps: int, fields_dev_ptr: int,
                   stream: int = 0) -> int:
@@ -248,6 +294,28 @@ def relax_noalloc(params: Params, Nx: int, Ny: int, dx: float, dy: float, nsteps
     L = load()
     return L.pfcg_relax_noalloc(ctypes.byref(params), Nx, Ny, dx, dy, nsteps, ctypes.c_void_p(fields_dev_ptr),
                                 ctypes.c_void_p(stream))
+
+
+class Hetero(ctypes.Structure):
+    """pfcg_hetero: a seeded two-field heterostructure initial state."""
+    _fields_ = [("grains", ctypes.c_int), ("stripe_width", ctypes.c_int), ("stripe_offset", ctypes.c_int),
+                ("sym", ctypes.c_int), ("mean", ctypes.c_double * 2), ("amp", ctypes.c_double * 2),
+                ("lattice", ctypes.c_double * 2), ("noise", ctypes.c_double), ("max_angle_deg", ctypes.c_double),
+                ("seed", ctypes.c_uint)]
+
+
+def make_hetero(grains: int, width: int, offset: int, means, amps, lattice, noise: float, seed: int,
+                sym: int = 3, max_angle_deg: float = 60.0) -> Hetero:
+    return Hetero(grains, width, offset, sym, (ctypes.c_double * 2)(*means), (ctypes.c_double * 2)(*amps),
+                  (ctypes.c_double * 2)(*lattice), noise, max_angle_deg, seed)
+
+
+def init_hetero(d_fields_ptr: int, Nx: int, Ny: int, dx: float, dy: float, spec: Hetero, stream: int = 0) -> None:
+    """pfcg_init_hetero into 2*Ny*Nx doubles of DEVICE memory."""
+    L = load()
+    rc = L.pfcg_init_hetero(ctypes.c_void_p(d_fields_ptr), Nx, Ny, dx, dy, ctypes.byref(spec), ctypes.c_void_p(stream))
+    if rc:
+        raise PfcError(rc, L.pfcg_init_last_error().decode())
 
 
 def last_error() -> str:

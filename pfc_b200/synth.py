@@ -141,3 +141,43 @@ def stripes2(Nx: int, Ny: int, dx: float, dy: float, width: int, means: tuple, a
         if noise:
             out[u] += noise * normal(seed, Nx * Ny, stream=3 + u).reshape(Ny, Nx)
     return out
+
+
+def hetero2(Nx: int, Ny: int, dx: float, dy: float, grains: int, width: int, offset: int, means: tuple,
+            amps: tuple, lattice: tuple, noise: float, seed: int, sym: int = 3,
+            max_angle_deg: float = 60.0) -> np.ndarray:
+    """Two-field heterostructure: each region belongs to one field, which carries
+    means[u] + amps[u] * OMA(r rotated by the region's angle, sym, lattice[u])
+    there, while the other field sits at its mean; noise * N(0, 1) is added to
+    both (streams 3 and 4). grains > 0: periodic Voronoi grains whose centre,
+    angle in [0, max_angle_deg) and field come from uniforms 4k..4k+3 of stream 1;
+    grains <= 0: vertical stripes, field ((x + offset) // width) % 2, unrotated.
+    With grains = 0 and offset = 0 this is stripes2. The device generator
+    pfcg_init_hetero computes the same values. Shape (2, Ny, Nx)."""
+    X = np.broadcast_to(np.arange(Nx)[None, :] * dx, (Ny, Nx))
+    Y = np.broadcast_to(np.arange(Ny)[:, None] * dy, (Ny, Nx))
+    if grains <= 0:
+        phase = np.broadcast_to(((np.arange(Nx)[None, :] + offset) // width) % 2, (Ny, Nx))
+        XR, YR = X, Y
+    else:
+        u = uniform(seed, 4 * grains, stream=1)
+        cx = u[0::4] * Nx * dx
+        cy = u[1::4] * Ny * dy
+        theta = u[2::4] * math.radians(max_angle_deg)
+        field = (u[3::4] >= 0.5).astype(np.int64)
+        lab = voronoi_labels(Nx, Ny, dx, dy, cx, cy)
+        phase = field[lab]
+        XR = np.empty((Ny, Nx))
+        YR = np.empty((Ny, Nx))
+        for n in range(grains):
+            sel = lab == n
+            c, s = math.cos(-theta[n]), math.sin(-theta[n])
+            XR[sel] = X[sel] * c - Y[sel] * s
+            YR[sel] = X[sel] * s + Y[sel] * c
+    out = np.empty((2, Ny, Nx))
+    for f in range(2):
+        lat = means[f] + amps[f] * oma(XR, YR, sym, lattice[f])
+        out[f] = np.where(phase == f, lat, means[f])
+        if noise:
+            out[f] += noise * normal(seed, Nx * Ny, stream=3 + f).reshape(Ny, Nx)
+    return out
