@@ -246,6 +246,63 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def run_ttr(args):
+    """Time to relaxed on the 4096^2 two-field workload: steps until the mean
+    free energy changes by less than 1e-9 per step over a 100-step window,
+    with the wall time of the whole run (every step and evaluation, and for the
+    warm start the network's tiled application). Three arms from the same
+    initial state: the plain FP64 iteration (the judge), the plain FP32
+    iteration, and FP32 after the learned warm start. Creating the network and
+    loading its weights is reported apart, as set-up."""
+    import torch
+
+    from pfc_b200 import fno
+
+    lib.set_device(0)
+    N = args.size
+    pd, dx, dy, f0 = workload(N, 0)
+    params = P.make_params(pd, 1.0, 0.25)
+    arms = {}
+    for name, prec, warm in (("plain_fp64", "fp64", False), ("plain_fp32", "fp32", False),
+                             ("warm_fp32", "fp32", True)):
+        r = lib.Relaxation(params, N, N, dx, dy, prec)
+        r.upload(f0)
+        rec = {}
+        net = None
+        if warm:
+            t0 = time.perf_counter()
+            meta = fno.weights_meta()
+            net = fno.Network(meta["tile"], 32)
+            net.set_params(fno.load_weights())
+            torch.cuda.synchronize()
+            rec["setup_s"] = time.perf_counter() - t0
+            rec["weights"] = {k: meta[k] for k in ("tile", "horizon", "pairs", "epochs") if k in meta}
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if warm:
+            r.warmstart(net)
+            torch.cuda.synchronize()
+            rec["network_s"] = time.perf_counter() - t0
+            rec["f_after_network"] = r.evaluate()[0]
+        steps, fave, _ = r.relax_until(1e-9, 100, args.ttr_max_steps)
+        rec.update(seconds=time.perf_counter() - t0, steps=steps, fave=fave, relaxed=steps is not None)
+        arms[name] = rec
+        r.close()
+        if net:
+            net.close()
+    f64 = arms["plain_fp64"]
+    for rec in arms.values():
+        rec["rel_dF_vs_plain_fp64"] = abs(rec["fave"] - f64["fave"]) / abs(f64["fave"])
+        rec["speedup_vs_plain_fp64"] = f64["seconds"] / rec["seconds"]
+    line = {"metric": "time to relaxed (|d<f>|/step < 1e-9), %dx%d two-field heterostructure" % (N, N),
+            "value": arms["warm_fp32"]["seconds"], "unit": "s", "higher_is_better": False,
+            "dtype": "f32", "data": "synthetic", "n_gpus": 1,
+            "config": {"workload": "hetero2c_%dx%d" % (N, N), "criterion": "|<f>(t) - <f>(t-100)| / 100 < 1e-9",
+                       "evaluate_every": 100},
+            "arms": arms}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -260,6 +317,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT reference timing")
     ap.add_argument("--batch", action="store_true", help="the batched workload (96 mixed problems) instead")
+    ap.add_argument("--ttr", action="store_true", help="time to relaxed: plain FP64, plain FP32, warm-started FP32")
+    ap.add_argument("--ttr-max-steps", type=int, default=80000)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -271,6 +330,10 @@ def main():
     if args.batch:
         lib.set_device(local)
         run_batch(args)
+        return
+    if args.ttr:
+        if rank == 0:
+            run_ttr(args)
         return
     if args.warmup < 3:
         args.warmup = 3

@@ -164,6 +164,87 @@ template <typename T, int U> struct StepConsts {
 	}
 };
 
+// ETD coefficients of one (kx, ky) entry (pfc-relax.c:940-955 and the coupling
+// terms of :1215-1244): A_u = exp(o a_u dt) and B_u (FP32: o dt phi1(o a_u dt);
+// FP64: the reference's (A - 1)/a, o dt at a = 0) for every field, and the
+// coupling coefficient beta_uv (mu2_uv - k2)^2 + eps_uv G^2 of every pair u < v.
+template <typename T, int U> __host__ __device__ constexpr int npairs() { return U * (U - 1) / 2 > 0 ? U * (U - 1) / 2 : 1; }
+template <typename T, int U>
+__device__ __forceinline__ void entry_coef(const StepConsts<T, U>& K, T k2, T (&A)[U], T (&Bn)[U],
+                                           T (&cu)[npairs<T, U>()]) {
+	if constexpr (U > 1) {
+		const T G = expT<T>(K.ag * k2);
+		const T G2 = G * G;
+		int p = 0;
+#pragma unroll
+		for (int u = 0; u < U - 1; u++)
+#pragma unroll
+			for (int v = u + 1; v < U; v++) {
+				T d2 = K.mu2[u][v] - k2;
+				d2 *= d2;
+				cu[p++] = K.beta[u][v] * d2 + K.eps[u][v] * G2;
+			}
+	}
+	const T o = K.cc - (T)1 - K.cc * k2;
+#pragma unroll
+	for (int u = 0; u < U; u++) {
+		T P = (T)1;
+#pragma unroll
+		for (int w = 0; w < MAXW; w++)
+			if (w < K.W[u]) {
+				const T q = K.nu2[u][w] - k2;
+				P *= K.omega[u][w] * q * q + K.phi[u][w];
+			}
+		const T av = K.alpha[u] + K.betad[u] * P;
+		const T x = o * av * K.dt;
+		A[u] = expT<T>(x);
+		if constexpr (sizeof(T) == 4) Bn[u] = o * K.dt * phi1f(x, A[u]);
+		else Bn[u] = (av == (T)0) ? o * K.dt : etd_b<T>(A[u], x, av);
+	}
+}
+
+// k^2 of entry (kx, ky) as the y-pass STEP computes it
+template <typename T>
+__device__ __forceinline__ T step_k2(int kx, int ky, int Ny, T dkxT, T dkyT, const Geom& g) {
+	if constexpr (sizeof(T) == 4) return k2_step<T>(kx, ky, Ny, dkxT, dkyT);
+	else return (T)k2_of(kx, ky, g, g.dx, g.dy);
+}
+
+// Coefficient table of the current box: the values entry_coef gives, so that
+// the STEP update reads 2U + U(U-1)/2 numbers per entry instead of evaluating
+// three exponentials and a quotient every step.
+template <typename T, int U>
+__global__ void __launch_bounds__(256) coef_kernel(Model m, Geom g, T* __restrict__ coef, long long cstride) {
+	const StepConsts<T, U> K(m, g.Nx, g.Ny);
+	const T dkxT = (T)g.dkx, dkyT = (T)g.dky;
+	const long long n = (long long)g.H * g.Ny;
+	for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+		const int kx = (int)(e / g.Ny), ky = (int)(e - (long long)kx * g.Ny);
+		T A[U], Bn[U], cu[npairs<T, U>()];
+		entry_coef<T, U>(K, step_k2<T>(kx, ky, g.Ny, dkxT, dkyT, g), A, Bn, cu);
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			coef[u * cstride + e] = A[u];
+			coef[(U + u) * cstride + e] = Bn[u];
+		}
+#pragma unroll
+		for (int p = 0; p < U * (U - 1) / 2; p++) coef[(2 * U + p) * cstride + e] = cu[p];
+	}
+}
+
+template <typename T>
+cudaError_t launch_coef(const Model& m, const Geom& g, int U, T* coef, long long cstride, cudaStream_t s) {
+	const long long n = (long long)g.H * g.Ny;
+	const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+	switch (U) {
+	case 1: coef_kernel<T, 1><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
+	case 2: coef_kernel<T, 2><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
+	case 3: coef_kernel<T, 3><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
+	default: coef_kernel<T, 4><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
+	}
+	return cudaGetLastError();
+}
+
 // Hermitian projection of one resident column (kx = 0 or kx = Nx/2): entry ky
 // and entry Ny - ky become (a + conj b)/2 and its conjugate, self-conjugate
 // entries become real. Writes shared memory and the spectral state. This is
@@ -754,42 +835,36 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 		const T dkxT = (T)a.g.dkx, dkyT = (T)a.g.dky;
 		// update of one (kx, ky) entry for all fields, pfc-relax.c:1215-1244
 		auto update = [&](int c, int kx, int ky, const cplx<T>(&Nv)[U]) {
-			const T k2 = (sizeof(T) == 4) ? k2_step<T>(kx, ky, Ny, dkxT, dkyT) : (T)k2_of(kx, ky, a.g, dx, dy);
+			T A[U], Bn[U], cu[npairs<T, U>()];
+			if (a.coef) {
+				const long long ci = (long long)kx * Ny + ky;
+#pragma unroll
+				for (int u = 0; u < U; u++) {
+					A[u] = __ldg(a.coef + u * a.cstride + ci);
+					Bn[u] = __ldg(a.coef + (U + u) * a.cstride + ci);
+				}
+#pragma unroll
+				for (int p = 0; p < U * (U - 1) / 2; p++) cu[p] = __ldg(a.coef + (2 * U + p) * a.cstride + ci);
+			} else {
+				entry_coef<T, U>(K, step_k2<T>(kx, ky, Ny, dkxT, dkyT, a.g), A, Bn, cu);
+			}
 			cplx<T> Mv[U];
 #pragma unroll
 			for (int u = 0; u < U; u++) Mv[u] = cscale(sm[(u * CC + c) * ld + pad<T>(ky)], K.invN);
 			if constexpr (U > 1) {
-				const T G = expT<T>(K.ag * k2);
-				const T G2 = G * G;
+				int p = 0;
 #pragma unroll
 				for (int u = 0; u < U - 1; u++)
 #pragma unroll
-					for (int v = u + 1; v < U; v++) {
-						T d2 = K.mu2[u][v] - k2;
-						d2 *= d2;
-						const T cu = K.beta[u][v] * d2 + K.eps[u][v] * G2;
-						Mv[u] = cadd(Mv[u], cscale(Nv[v], cu));
-						Mv[v] = cadd(Mv[v], cscale(Nv[u], cu));
+					for (int v = u + 1; v < U; v++, p++) {
+						Mv[u] = cadd(Mv[u], cscale(Nv[v], cu[p]));
+						Mv[v] = cadd(Mv[v], cscale(Nv[u], cu[p]));
 					}
 			}
 			const bool origin = (kx == 0 && ky == 0);
-			const T o = K.cc - (T)1 - K.cc * k2;
 #pragma unroll
 			for (int u = 0; u < U; u++) {
-				T P = (T)1;
-#pragma unroll
-				for (int w = 0; w < MAXW; w++)
-					if (w < K.W[u]) {
-						const T q = K.nu2[u][w] - k2;
-						P *= K.omega[u][w] * q * q + K.phi[u][w];
-					}
-				const T av = K.alpha[u] + K.betad[u] * P;
-				const T x = o * av * K.dt;
-				const T A = expT<T>(x);
-				T Bn;
-				if constexpr (sizeof(T) == 4) Bn = o * K.dt * phi1f(x, A);
-				else Bn = (av == (T)0) ? o * K.dt : etd_b<T>(A, x, av);
-				cplx<T> nn = cadd(cscale(Nv[u], A), cscale(Mv[u], Bn));
+				cplx<T> nn = cadd(cscale(Nv[u], A[u]), cscale(Mv[u], Bn[u]));
 				if (origin) nn = mk<T>((T)0, (T)0);
 				a.spec[u * a.sstride + (long long)kx * Ny + ky] = nn;
 				sm[(u * CC + c) * ld + pad<T>(ky)] = nn;
