@@ -252,7 +252,8 @@ def run_ttr(args):
     with the wall time of the whole run (every step and evaluation, and for the
     warm start the network's tiled application). Three arms from the same
     initial state: the plain FP64 iteration (the judge), the plain FP32
-    iteration, and FP32 after the learned warm start. Creating the network and
+    iteration, and FP32 with the learned warm start (the network's input step of
+    plain steps, the network, then the plain finish). Creating the network and
     loading its weights is reported apart, as set-up."""
     import torch
 
@@ -276,16 +277,23 @@ def run_ttr(args):
             net.set_params(fno.load_weights())
             torch.cuda.synchronize()
             rec["setup_s"] = time.perf_counter() - t0
-            rec["weights"] = {k: meta[k] for k in ("tile", "horizon", "pairs", "epochs") if k in meta}
+            rec["weights"] = {k: meta[k] for k in ("tile", "input_step", "horizon", "pairs", "epochs", "val_mse",
+                                                   "identity_mse") if k in meta}
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        pre = 0
         if warm:
+            # the network's input is the state after its input step of plain FP32 steps
+            pre = int(meta.get("input_step", 0))
+            r.step(pre)
+            t1 = time.perf_counter()
             r.warmstart(net)
             torch.cuda.synchronize()
-            rec["network_s"] = time.perf_counter() - t0
+            rec["network_s"] = time.perf_counter() - t1
             rec["f_after_network"] = r.evaluate()[0]
         steps, fave, _ = r.relax_until(1e-9, 100, args.ttr_max_steps)
-        rec.update(seconds=time.perf_counter() - t0, steps=steps, fave=fave, relaxed=steps is not None)
+        rec.update(seconds=time.perf_counter() - t0, steps=None if steps is None else steps + pre, fave=fave,
+                   relaxed=steps is not None, plain_steps_before_network=pre)
         arms[name] = rec
         r.close()
         if net:

@@ -71,9 +71,7 @@ struct pfcg_handle {
 	double* d_real = nullptr;   // U*Ny*Nx doubles
 	double* d_fields = nullptr; // f(r) work fields
 	double* d_part = nullptr;   // partial sums of the field means
-	void* coef = nullptr;       // per-entry ETD coefficients of the STEP update (coef_planes(U) planes)
-	double coef_dx = 0.0, coef_dy = 0.0; // box the table was built for (0: not built)
-	bool use_coef = true;       // PFCG_COEF_TABLES=0 computes them in the y-pass instead
+	int ahead_x = 0, ahead_y = 0; // L2 prefetch distance of the specialised STEP kernels (resident CTAs)
 	long long launches = 0;
 	// per-kernel timing (pfcg_set_profiling)
 	bool profiling = false;
@@ -226,9 +224,6 @@ int choose_layout(pfcg_handle* h, int nsm) {
 		if (h->Ny / r >= want) break;
 	}
 	if (!R) return fail(h, PFCG_ESIZE, "no x-pass tile fits shared memory for this Nx");
-	// PFCG_COEF_TABLES=0 evaluates the ETD coefficients in the y-pass every step (A/B checks)
-	const char* ct = std::getenv("PFCG_COEF_TABLES");
-	h->use_coef = !(ct && ct[0] == '0');
 	int CC = 0;
 	const bool yspec = allow_spec && spec_cols(fp64, U, h->Ny) && spec_rows(fp64, U, h->Ny) == R;
 	if (yspec) CC = spec_cols(fp64, U, h->Ny);
@@ -240,7 +235,13 @@ int choose_layout(pfcg_handle* h, int nsm) {
 	}
 	if (!CC) return fail(h, PFCG_ESIZE, "no y-pass column group fits shared memory for this Ny");
 	set_generic_configs(h, R, CC);
-	if (rs && R == rs) h->cxs = {h->Ny / R, spec_x_threads(fp64, U, h->Nx), spec_x_smem(fp64, U, h->Nx), 1};
+	// PFCG_L2_PREFETCH=0 switches off the next-wave L2 prefetch of the specialised STEP kernels
+	const char* pf = std::getenv("PFCG_L2_PREFETCH");
+	const int resident = (pf && pf[0] == '0') ? 0 : nsm * (fp64 ? 1 : 2);
+	if (rs && R == rs) {
+		h->cxs = {h->Ny / R, spec_x_threads(fp64, U, h->Nx), spec_x_smem(fp64, U, h->Nx), 1};
+		h->ahead_x = resident;
+	}
 	if (yspec) {
 		// The specialised y-pass keeps the update between the two transforms in
 		// shared memory by default (measured faster at 4096^2 U=2: 0.299 vs 0.328 ms);
@@ -248,6 +249,7 @@ int choose_layout(pfcg_handle* h, int nsm) {
 		const char* fu = std::getenv("PFCG_YPASS_FUSED");
 		const bool fused = fu && fu[0] == '1';
 		h->cys = {(h->H + CC - 1) / CC, spec_y_threads(fp64, U, h->Ny, fused), spec_y_smem(fp64, U, h->Ny), fused ? 1 : 2};
+		h->ahead_y = resident;
 	}
 	return 0;
 }
@@ -357,6 +359,7 @@ template <typename T> XArgs<T> xargs(pfcg_handle* h) {
 	a.sb = h->sbx;
 	a.m = h->model;
 	a.g = h->geom;
+	a.ahead = h->ahead_x;
 	return a;
 }
 
@@ -374,23 +377,8 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.sb = h->sby;
 	a.m = h->model;
 	a.g = h->geom;
-	const bool fresh = h->coef && h->coef_dx == h->geom.dx && h->coef_dy == h->geom.dy;
-	a.coef = fresh ? (const T*)h->coef : nullptr;
-	a.cstride = (long long)h->H * h->Ny;
+	a.ahead = h->ahead_y;
 	return a;
-}
-
-// (Re)builds the coefficient table when the box changed since it was built.
-template <typename T> int ensure_coef(pfcg_handle* h) {
-	if (!h->use_coef) return 0;
-	if (h->coef && h->coef_dx == h->geom.dx && h->coef_dy == h->geom.dy) return 0;
-	const long long cs = (long long)h->H * h->Ny;
-	if (!h->coef) CK(h, cudaMalloc(&h->coef, sizeof(T) * coef_planes(h->U) * cs));
-	h->launches++;
-	CK(h, launch_coef<T>(h->model, h->geom, h->U, (T*)h->coef, cs, h->stream));
-	h->coef_dx = h->geom.dx;
-	h->coef_dy = h->geom.dy;
-	return 0;
 }
 
 constexpr int MEAN_BLOCKS = 296;
@@ -506,8 +494,6 @@ template <typename T> int do_download(pfcg_handle* h, double* fields, cudaMemcpy
 }
 
 template <typename T> int do_steps(pfcg_handle* h, int nsteps) {
-	int rc0 = ensure_coef<T>(h);
-	if (rc0) return rc0;
 	XArgs<T> xa = xargs<T>(h);
 	xa.acc = h->acc + ACC_NL;
 	YArgs<T> ya = yargs<T>(h);
@@ -785,7 +771,6 @@ void pfcg_destroy(pfcg_handle* h) {
 	cudaFree(h->d_real);
 	cudaFree(h->d_fields);
 	cudaFree(h->d_part);
-	cudaFree(h->coef);
 	for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
 	if (h->h_flag) cudaFreeHost(h->h_flag);
 	if (h->h_buf) cudaFreeHost(h->h_buf);
@@ -1011,7 +996,6 @@ template <typename T> int batch_build(pfcg_batch* b) {
 		xa[i].acc = h->acc + ACC_NL;
 		xa[i].flag = b->d_flags + i;
 		ya[i] = yargs<T>(h);
-		ya[i].coef = nullptr; // a batch problem's box may change between steps: compute in the kernel
 		b->threads = std::max(b->threads, std::max(h->cx.block, h->cy.block));
 		b->smem = std::max(b->smem, std::max(h->cx.smem, h->cy.smem));
 	}
@@ -1305,7 +1289,6 @@ extern "C" int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double d
 	CKN(launch_field_means(fields, h.U, (long long)Nx * Ny, h.d_part, MEAN_BLOCKS, h.mean, h.stream));
 	XArgs<float> xa = xargs<float>(&h);
 	YArgs<float> ya = yargs<float>(&h);
-	ya.coef = nullptr;
 	if ((rc = run_xpass<float>(&h, XP_R2C, xa, h.cx))) return done(rc);
 	if ((rc = run_ypass<float>(&h, YP_INIT, ya, h.cy))) return done(rc);
 	xa.acc = h.acc + ACC_NL;

@@ -69,6 +69,7 @@ template <typename T> struct XArgs {
 	int sb;                 // channel pairs per FFT call
 	Model m;
 	Geom g;
+	int ahead;              // STEP: L2 prefetch of the tile of block + ahead (0 = none)
 };
 
 // Parameters of one k-space weight (YP_WEIGHT), resolved on the host so the
@@ -94,13 +95,8 @@ template <typename T> struct YArgs {
 	Geom g;
 	int wkind, wsrc;        // YP_WEIGHT: weight kind and source field
 	WParams wp;             // YP_WEIGHT: parameters of the weight
-	const T* coef;          // YP_STEP: per-entry ETD coefficients (coef_planes(U) planes), or NULL to compute them
-	long long cstride;      // plane stride of coef (H * Ny)
+	int ahead;              // STEP: L2 prefetch of the column group of block + ahead (0 = none)
 };
-
-// Planes of the per-entry coefficient table of the STEP update: A_u, B_u for
-// every field, then the coupling coefficient of every pair u < v.
-inline int coef_planes(int U) { return 2 * U + U * (U - 1) / 2; }
 
 struct LaunchCfg {
 	int grid, block, smem;
@@ -129,11 +125,6 @@ template <typename T>
 cudaError_t launch_batch_step(const XArgs<T>* xprobs, const YArgs<T>* yprobs, const int* xblk_prob, const int* xblk_local,
                               int xblocks, const int* yblk_prob, const int* yblk_local, int yblocks, int threads, int smem,
                               cudaStream_t s);
-
-// Fills the coefficient table of the current box (coef_planes(U) planes of
-// cstride entries, [kx][ky] order like the spectral state).
-template <typename T>
-cudaError_t launch_coef(const Model& m, const Geom& g, int U, T* coef, long long cstride, cudaStream_t s);
 
 // Parseval sums for up to MAX_TRIAL box sizes (see kernels.cu): out[t] += ...
 template <typename T>

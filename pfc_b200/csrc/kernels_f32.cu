@@ -12,6 +12,5 @@ template cudaError_t launch_batch_step<float>(const XArgs<float>*, const YArgs<f
                                             const int*, int, int, int, cudaStream_t);
 
 template void prepare_batch_kernels<float>();
-template cudaError_t launch_coef<float>(const Model&, const Geom&, int, float*, long long, cudaStream_t);
 
 } // namespace pfcg

@@ -12,6 +12,5 @@ template cudaError_t launch_batch_step<double>(const XArgs<double>*, const YArgs
                                             const int*, int, int, int, cudaStream_t);
 
 template void prepare_batch_kernels<double>();
-template cudaError_t launch_coef<double>(const Model&, const Geom&, int, double*, long long, cudaStream_t);
 
 } // namespace pfcg

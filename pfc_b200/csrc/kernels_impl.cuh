@@ -164,6 +164,14 @@ template <typename T, int U> struct StepConsts {
 	}
 };
 
+// L2 prefetch hints. A CTA of a STEP pass asks L2 for the data of the CTA
+// expected to start one wave after it (block + number of resident CTAs), so the
+// DRAM latency of the next wave's loads overlaps this wave's transforms.
+__device__ __forceinline__ void l2_prefetch_bulk(const void* p, unsigned bytes) {
+	asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void l2_prefetch_line(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ETD coefficients of one (kx, ky) entry (pfc-relax.c:940-955 and the coupling
 // terms of :1215-1244): A_u = exp(o a_u dt) and B_u (FP32: o dt phi1(o a_u dt);
 // FP64: the reference's (A - 1)/a, o dt at a = 0) for every field, and the
@@ -208,41 +216,6 @@ template <typename T>
 __device__ __forceinline__ T step_k2(int kx, int ky, int Ny, T dkxT, T dkyT, const Geom& g) {
 	if constexpr (sizeof(T) == 4) return k2_step<T>(kx, ky, Ny, dkxT, dkyT);
 	else return (T)k2_of(kx, ky, g, g.dx, g.dy);
-}
-
-// Coefficient table of the current box: the values entry_coef gives, so that
-// the STEP update reads 2U + U(U-1)/2 numbers per entry instead of evaluating
-// three exponentials and a quotient every step.
-template <typename T, int U>
-__global__ void __launch_bounds__(256) coef_kernel(Model m, Geom g, T* __restrict__ coef, long long cstride) {
-	const StepConsts<T, U> K(m, g.Nx, g.Ny);
-	const T dkxT = (T)g.dkx, dkyT = (T)g.dky;
-	const long long n = (long long)g.H * g.Ny;
-	for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-		const int kx = (int)(e / g.Ny), ky = (int)(e - (long long)kx * g.Ny);
-		T A[U], Bn[U], cu[npairs<T, U>()];
-		entry_coef<T, U>(K, step_k2<T>(kx, ky, g.Ny, dkxT, dkyT, g), A, Bn, cu);
-#pragma unroll
-		for (int u = 0; u < U; u++) {
-			coef[u * cstride + e] = A[u];
-			coef[(U + u) * cstride + e] = Bn[u];
-		}
-#pragma unroll
-		for (int p = 0; p < U * (U - 1) / 2; p++) coef[(2 * U + p) * cstride + e] = cu[p];
-	}
-}
-
-template <typename T>
-cudaError_t launch_coef(const Model& m, const Geom& g, int U, T* coef, long long cstride, cudaStream_t s) {
-	const long long n = (long long)g.H * g.Ny;
-	const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
-	switch (U) {
-	case 1: coef_kernel<T, 1><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
-	case 2: coef_kernel<T, 2><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
-	case 3: coef_kernel<T, 3><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
-	default: coef_kernel<T, 4><<<grid, 256, 0, s>>>(m, g, coef, cstride); break;
-	}
-	return cudaGetLastError();
 }
 
 // Hermitian projection of one resident column (kx = 0 or kx = Nx/2): entry ky
@@ -331,6 +304,10 @@ __device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm,
 	constexpr int H = NC / 2 + 1;
 	constexpr int CH = U * RC;
 	const long long tofs = (long long)tile * H * RC;
+	// next wave's tile: U contiguous runs of H * RC elements (16-byte multiples)
+	if (a.ahead > 0 && tile + a.ahead < a.g.Ny / RC && (tid & 31) == 0 && (tid >> 5) < U)
+		l2_prefetch_bulk(a.work + (tid >> 5) * a.wstride + tofs + (long long)a.ahead * H * RC,
+		                 (unsigned)(sizeof(cplx<T>) * H * RC));
 	// Hermitian-extended pair spectra (as in the runtime kernel); the loop is
 	// unrolled so that all of a thread's loads are in flight together
 	constexpr int KIT = (H + NT - 1) / NT;
@@ -786,6 +763,22 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 		return;
 	}
 
+	if constexpr (C::CT && MODE == YP_STEP) {
+		// next wave's column group: its spectral columns (contiguous) and the
+		// RC-element chunks of its work columns, one line per chunk
+		const int g2 = grp + a.ahead;
+		if (a.ahead > 0 && g2 * CCC < H) {
+			const int c2 = min(CCC, H - g2 * CCC);
+			if ((tid & 31) == 0 && (tid >> 5) < U)
+				l2_prefetch_bulk(a.spec + (tid >> 5) * a.sstride + (long long)g2 * CCC * NC,
+				                 (unsigned)(sizeof(cplx<T>) * c2 * NC));
+#pragma unroll
+			for (int u = 0; u < U; u++)
+				for (int t = tid; t < NC / RC; t += C::NT)
+					l2_prefetch_line(a.work + u * a.wstride + t * tileH + (long long)g2 * CCC * RC);
+		}
+	}
+
 	if constexpr (MODE != YP_WEIGHT) {
 		if constexpr (C::CT && ((NC / RC) * CCC * RC) % C::NT == 0) {
 			// every load of the tile in flight before the first shared-memory store
@@ -836,18 +829,7 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 		// update of one (kx, ky) entry for all fields, pfc-relax.c:1215-1244
 		auto update = [&](int c, int kx, int ky, const cplx<T>(&Nv)[U]) {
 			T A[U], Bn[U], cu[npairs<T, U>()];
-			if (a.coef) {
-				const long long ci = (long long)kx * Ny + ky;
-#pragma unroll
-				for (int u = 0; u < U; u++) {
-					A[u] = __ldg(a.coef + u * a.cstride + ci);
-					Bn[u] = __ldg(a.coef + (U + u) * a.cstride + ci);
-				}
-#pragma unroll
-				for (int p = 0; p < U * (U - 1) / 2; p++) cu[p] = __ldg(a.coef + (2 * U + p) * a.cstride + ci);
-			} else {
-				entry_coef<T, U>(K, step_k2<T>(kx, ky, Ny, dkxT, dkyT, a.g), A, Bn, cu);
-			}
+			entry_coef<T, U>(K, step_k2<T>(kx, ky, Ny, dkxT, dkyT, a.g), A, Bn, cu);
 			cplx<T> Mv[U];
 #pragma unroll
 			for (int u = 0; u < U; u++) Mv[u] = cscale(sm[(u * CC + c) * ld + pad<T>(ky)], K.invN);

@@ -7,10 +7,19 @@ the parameter initialisation, the weight file, data generation (seeded
 initial states from pfcg_init_hetero, relaxed by the batched FP32 path) and
 the training loop. torch provides device buffers and index shuffling only.
 
+The shipped weights (weights/fno_hetero2c_512.npz, made by `python -m
+pfc_b200.fno`) map the state after `input_step` (500) plain FP32 steps to the
+state `horizon` (4500) steps later; the seeded initial state itself is not a
+usable input, because the lattice that forms in the first few hundred steps is
+not predictable from it (the state after 2000 steps is as far from the initial
+one as the fully relaxed state is).
+
 Usage:
-    net = Network(tile=512, max_batch=16)
-    net.set_params(load_weights(DEFAULT_WEIGHTS))
+    net = Network(tile=512, max_batch=32)
+    net.set_params(load_weights())
+    relaxation.step(weights_meta()["input_step"])
     relaxation.warmstart(net)         # pfcg_warmstart on a U = 2 handle
+    relaxation.relax_until(1e-9)      # the plain method finishes and judges
 """
 from __future__ import annotations
 
@@ -293,3 +302,40 @@ def evaluate_mse(net: Network, X, Y, batch: int = 16) -> float:
 
 def identity_mse(X, Y) -> float:
     return float(((X - Y) ** 2).mean())
+
+
+def main(argv=None) -> None:
+    """Regenerates the shipped weights: python -m pfc_b200.fno [--pairs 4000 ...].
+    Input = the state after --input-step plain FP32 steps, target = the state
+    after --target-step steps, 512 x 512 two-field heterostructures."""
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=4000)
+    ap.add_argument("--input-step", type=int, default=500)
+    ap.add_argument("--target-step", type=int, default=5000)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    a = ap.parse_args(argv)
+    X0, Ys = make_pairs(a.pairs, 512, (a.input_step, a.target_step), seed0=a.seed, chunk=500)
+    X, Y = Ys[a.input_step], Ys[a.target_step]
+    del X0
+    nval = 96
+    with Network(512, a.batch) as net:
+        net.set_params(init_params(0))
+        tr = train(net, X[:-nval], Y[:-nval], epochs=a.epochs, batch=a.batch, lr=a.lr,
+                   val=(X[-nval:], Y[-nval:]))
+        save_weights(a.out, net.get_params(),
+                     {"tile": 512, "input_step": a.input_step, "horizon": a.target_step - a.input_step,
+                      "pairs": a.pairs, "epochs": a.epochs, "val_mse": tr["history"][-1]["val_mse"],
+                      "identity_mse": identity_mse(X[-nval:], Y[-nval:]), "batch": a.batch, "lr": a.lr,
+                      "data": "fno.make_pairs(%d, 512, (%d, %d), seed0=%d): state after %d FP32 steps -> state after %d"
+                              % (a.pairs, a.input_step, a.target_step, a.seed, a.input_step, a.target_step),
+                      "model": "hetero_2c(0.04), c=1, dt=0.25, dx=dy=0.7"})
+
+
+if __name__ == "__main__":
+    main()
