@@ -71,7 +71,6 @@ struct pfcg_handle {
 	double* d_real = nullptr;   // U*Ny*Nx doubles
 	double* d_fields = nullptr; // f(r) work fields
 	double* d_part = nullptr;   // partial sums of the field means
-	int ahead_x = 0, ahead_y = 0; // L2 prefetch distance of the specialised STEP kernels (resident CTAs)
 	long long launches = 0;
 	// per-kernel timing (pfcg_set_profiling)
 	bool profiling = false;
@@ -235,13 +234,7 @@ int choose_layout(pfcg_handle* h, int nsm) {
 	}
 	if (!CC) return fail(h, PFCG_ESIZE, "no y-pass column group fits shared memory for this Ny");
 	set_generic_configs(h, R, CC);
-	// PFCG_L2_PREFETCH=0 switches off the next-wave L2 prefetch of the specialised STEP kernels
-	const char* pf = std::getenv("PFCG_L2_PREFETCH");
-	const int resident = (pf && pf[0] == '0') ? 0 : nsm * (fp64 ? 1 : 2);
-	if (rs && R == rs) {
-		h->cxs = {h->Ny / R, spec_x_threads(fp64, U, h->Nx), spec_x_smem(fp64, U, h->Nx), 1};
-		h->ahead_x = resident;
-	}
+	if (rs && R == rs) h->cxs = {h->Ny / R, spec_x_threads(fp64, U, h->Nx), spec_x_smem(fp64, U, h->Nx), 1};
 	if (yspec) {
 		// The specialised y-pass keeps the update between the two transforms in
 		// shared memory by default (measured faster at 4096^2 U=2: 0.299 vs 0.328 ms);
@@ -249,7 +242,6 @@ int choose_layout(pfcg_handle* h, int nsm) {
 		const char* fu = std::getenv("PFCG_YPASS_FUSED");
 		const bool fused = fu && fu[0] == '1';
 		h->cys = {(h->H + CC - 1) / CC, spec_y_threads(fp64, U, h->Ny, fused), spec_y_smem(fp64, U, h->Ny), fused ? 1 : 2};
-		h->ahead_y = resident;
 	}
 	return 0;
 }
@@ -359,7 +351,6 @@ template <typename T> XArgs<T> xargs(pfcg_handle* h) {
 	a.sb = h->sbx;
 	a.m = h->model;
 	a.g = h->geom;
-	a.ahead = h->ahead_x;
 	return a;
 }
 
@@ -377,7 +368,6 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.sb = h->sby;
 	a.m = h->model;
 	a.g = h->geom;
-	a.ahead = h->ahead_y;
 	return a;
 }
 

@@ -69,7 +69,6 @@ template <typename T> struct XArgs {
 	int sb;                 // channel pairs per FFT call
 	Model m;
 	Geom g;
-	int ahead;              // STEP: L2 prefetch of the tile of block + ahead (0 = none)
 };
 
 // Parameters of one k-space weight (YP_WEIGHT), resolved on the host so the
@@ -95,7 +94,6 @@ template <typename T> struct YArgs {
 	Geom g;
 	int wkind, wsrc;        // YP_WEIGHT: weight kind and source field
 	WParams wp;             // YP_WEIGHT: parameters of the weight
-	int ahead;              // STEP: L2 prefetch of the column group of block + ahead (0 = none)
 };
 
 struct LaunchCfg {

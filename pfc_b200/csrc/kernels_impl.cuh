@@ -164,14 +164,6 @@ template <typename T, int U> struct StepConsts {
 	}
 };
 
-// L2 prefetch hints. A CTA of a STEP pass asks L2 for the data of the CTA
-// expected to start one wave after it (block + number of resident CTAs), so the
-// DRAM latency of the next wave's loads overlaps this wave's transforms.
-__device__ __forceinline__ void l2_prefetch_bulk(const void* p, unsigned bytes) {
-	asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void l2_prefetch_line(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
 // ETD coefficients of one (kx, ky) entry (pfc-relax.c:940-955 and the coupling
 // terms of :1215-1244): A_u = exp(o a_u dt) and B_u (FP32: o dt phi1(o a_u dt);
 // FP64: the reference's (A - 1)/a, o dt at a = 0) for every field, and the
@@ -304,10 +296,6 @@ __device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm,
 	constexpr int H = NC / 2 + 1;
 	constexpr int CH = U * RC;
 	const long long tofs = (long long)tile * H * RC;
-	// next wave's tile: U contiguous runs of H * RC elements (16-byte multiples)
-	if (a.ahead > 0 && tile + a.ahead < a.g.Ny / RC && (tid & 31) == 0 && (tid >> 5) < U)
-		l2_prefetch_bulk(a.work + (tid >> 5) * a.wstride + tofs + (long long)a.ahead * H * RC,
-		                 (unsigned)(sizeof(cplx<T>) * H * RC));
 	// Hermitian-extended pair spectra (as in the runtime kernel); the loop is
 	// unrolled so that all of a thread's loads are in flight together
 	constexpr int KIT = (H + NT - 1) / NT;
@@ -761,22 +749,6 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 	if constexpr (MODE == YP_STEP && C::FUSED && FUSEDK) {
 		ypass_step_fused<T, U, NC, CCC, RC, C::S, C::NT, MAXE>(a, sm, tws, kx0, ncol, tid);
 		return;
-	}
-
-	if constexpr (C::CT && MODE == YP_STEP) {
-		// next wave's column group: its spectral columns (contiguous) and the
-		// RC-element chunks of its work columns, one line per chunk
-		const int g2 = grp + a.ahead;
-		if (a.ahead > 0 && g2 * CCC < H) {
-			const int c2 = min(CCC, H - g2 * CCC);
-			if ((tid & 31) == 0 && (tid >> 5) < U)
-				l2_prefetch_bulk(a.spec + (tid >> 5) * a.sstride + (long long)g2 * CCC * NC,
-				                 (unsigned)(sizeof(cplx<T>) * c2 * NC));
-#pragma unroll
-			for (int u = 0; u < U; u++)
-				for (int t = tid; t < NC / RC; t += C::NT)
-					l2_prefetch_line(a.work + u * a.wstride + t * tileH + (long long)g2 * CCC * RC);
-		}
 	}
 
 	if constexpr (MODE != YP_WEIGHT) {
