@@ -71,6 +71,7 @@ struct pfcg_handle {
 	double* d_real = nullptr;   // U*Ny*Nx doubles
 	double* d_fields = nullptr; // f(r) work fields
 	double* d_part = nullptr;   // partial sums of the field means
+	int regio = 1;              // y-pass register ends (PFCG_YPASS_REGIO=0: load/store phases through shared memory)
 	long long launches = 0;
 	// per-kernel timing (pfcg_set_profiling)
 	bool profiling = false;
@@ -242,6 +243,8 @@ int choose_layout(pfcg_handle* h, int nsm) {
 		const char* fu = std::getenv("PFCG_YPASS_FUSED");
 		const bool fused = fu && fu[0] == '1';
 		h->cys = {(h->H + CC - 1) / CC, spec_y_threads(fp64, U, h->Ny, fused), spec_y_smem(fp64, U, h->Ny), fused ? 1 : 2};
+		const char* ri = std::getenv("PFCG_YPASS_REGIO");
+		h->regio = (ri && ri[0] == '0') ? 0 : 1;
 	}
 	return 0;
 }
@@ -368,6 +371,7 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.sb = h->sby;
 	a.m = h->model;
 	a.g = h->geom;
+	a.regio = h->regio;
 	return a;
 }
 

@@ -94,6 +94,7 @@ template <typename T> struct YArgs {
 	Geom g;
 	int wkind, wsrc;        // YP_WEIGHT: weight kind and source field
 	WParams wp;             // YP_WEIGHT: parameters of the weight
+	int regio;              // STEP, specialised kernels: first/last transform pass to/from global memory
 };
 
 struct LaunchCfg {

@@ -751,7 +751,41 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 		return;
 	}
 
-	if constexpr (MODE != YP_WEIGHT) {
+	// Register ends (STEP, one butterfly per thread per pass): the forward
+	// transform's first pass takes its inputs straight from global memory and
+	// the inverse transform's last pass stores straight to it, which saves the
+	// shared-memory round trip and barrier of a separate load and store phase.
+	constexpr int NCX = C::CT ? NC : 256;
+	using PLX = CtPlan<NCX, MAXE>;
+	constexpr bool REGIO = C::CT && MODE == YP_STEP && !(C::FUSED && FUSEDK) && C::NSUB == C::S &&
+	                       C::S * (NCX / MAXE) == C::NT && PLX::FUSABLE;
+	using RBY = RegBlock<NCX, MAXE, C::S, C::NT, T>;
+	// global address of element y of resident sequence p (field p / CCC, column p % CCC)
+	auto gaddr = [&](int p, int y) -> long long {
+		return (long long)(p / (C::CT ? CCC : 1)) * a.wstride + (long long)(y / RC) * tileH +
+		       (long long)(kx0 + p % (C::CT ? CCC : 1)) * RC + y % RC;
+	};
+	bool regio = false;
+	if constexpr (REGIO) {
+		if (a.regio) {
+			regio = true;
+			RBY rb;
+#pragma unroll
+			for (int i = 0; i < RBY::NB; i++) {
+				const int p = RBY::seq(tid, i);
+				const bool live = p % CCC < ncol;
+#pragma unroll
+				for (int r = 0; r < MAXE; r++)
+					rb.v[i][r] = live ? a.work[gaddr(p, RBY::pos(tid, i, r))] : mk<T>((T)0, (T)0);
+			}
+			ct_first_from_regs<NCX, MAXE, C::S, C::NT, -1, T>(sm, rb, tid);
+			ct_middle<NCX, MAXE, C::S, C::NT, -1, T>(sm, tws, tid);
+			ct_pass<NCX, PLX::radix(PLX::NPASS - 1), PLX::ns(PLX::NPASS - 1), PLX::twoff(PLX::NPASS - 1), C::S, C::NT,
+			        -1, T>(sm, tws, tid);
+		}
+	}
+
+	if constexpr (MODE != YP_WEIGHT) if (!regio) {
 		if constexpr (C::CT && ((NC / RC) * CCC * RC) % C::NT == 0) {
 			// every load of the tile in flight before the first shared-memory store
 			constexpr int CH = CCC * RC;
@@ -918,6 +952,23 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 		}
 	}
 	__syncthreads();
+	if constexpr (REGIO) {
+		if (regio) {
+			ct_pass<NCX, PLX::radix(0), PLX::ns(0), PLX::twoff(0), C::S, C::NT, +1, T>(sm, tws, tid);
+			ct_middle<NCX, MAXE, C::S, C::NT, +1, T>(sm, tws, tid);
+			RBY rb;
+			ct_last_to_regs<NCX, MAXE, C::S, C::NT, +1, T>(sm, tws, rb, tid);
+#pragma unroll
+			for (int i = 0; i < RBY::NB; i++) {
+				const int p = RBY::seq(tid, i);
+				if (p % CCC < ncol) {
+#pragma unroll
+					for (int r = 0; r < MAXE; r++) a.work[gaddr(p, RBY::pos(tid, i, r))] = rb.v[i][r];
+				}
+			}
+			return;
+		}
+	}
 	if constexpr (C::CT) fft_ct<NC, MAXE, C::S, C::NSUB, C::NT, +1, T>(sm, tws, tid);
 	else fft_batches<+1, MAXE, T>(sm, ld, S, a.sb, a.plan, a.tw, tid, nt);
 
