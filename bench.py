@@ -246,6 +246,24 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def accuracy_profile(params, N, dx, dy, f0, marks=(10, 100, 300)):
+    """FP32 against FP64 from the same initial state at fixed step counts:
+    relative difference of <f> and max |psi_fp32 - psi_fp64| over the grid."""
+    out = []
+    with lib.Relaxation(params, N, N, dx, dy, "fp32") as a, lib.Relaxation(params, N, N, dx, dy, "fp64") as b:
+        a.upload(f0)
+        b.upload(f0)
+        done = 0
+        for m in marks:
+            a.step(m - done)
+            b.step(m - done)
+            done = m
+            fa, fb = a.evaluate()[0], b.evaluate()[0]
+            da = float(np.abs(a.download() - b.download()).max())
+            out.append({"steps": m, "rel_dF": abs(fa - fb) / abs(fb), "max_dpsi": da})
+    return out
+
+
 def run_ttr(args):
     """Time to relaxed on the 4096^2 two-field workload: steps until the mean
     free energy changes by less than 1e-9 per step over a 100-step window,
@@ -464,6 +482,10 @@ def main():
         cufft = {"ms_r2c_plus_c2r": e0.elapsed_time(e1) / 20, "what": "torch.fft rfft2 + irfft2 of the U fields (cuFFT)"}
         del x, y
 
+    acc = None
+    if rank == 0 and not args.no_fp64 and main_p == "fp32":
+        acc = accuracy_profile(params, N, dx, dy, f0)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(N, U, rank, args.cpu_steps)
@@ -490,6 +512,8 @@ def main():
         r64 = results["fp64"]
         line["fp64"] = {"steps_per_s": args.steps * 1000.0 / r64["ms"] * world, "ms_per_step": r64["ms"] / args.steps,
                         "fave": r64["fave"], "rel_dF_vs_fp32": abs(res["fave"] - r64["fave"]) / abs(r64["fave"])}
+    if acc:
+        line["accuracy_fp32_vs_fp64"] = acc
     if cpu:
         line["cpu_baseline"] = cpu
     if cufft:

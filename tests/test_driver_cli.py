@@ -164,3 +164,46 @@ def test_full_run_matches_reference(tmp_path):
         np.testing.assert_allclose(np.array(gt[1:], float), np.array(rt[1:], float), rtol=0, atol=1e-8, err_msg=n)
         # number formatting: "%.12e" lines
         assert all(len(line.split("e")[0].split(".")[1]) == 12 for line in gt[1:50])
+
+
+def big_case(tmp_path, Nx, Ny, prec, values_text):
+    text = GOOD_1C.replace("\t10\t[\t0\t20\t]\t12\t6", "\t10\t[\t0\t20\t]\t12\t%d" % prec)
+    (tmp_path / "x.in").write_text(text)
+    (tmp_path / "in0.n").write_text("%d %d 0.785 0.785\n" % (Nx, Ny) + values_text)
+
+
+@pytest.mark.parametrize("threads,prec", [(1, 6), (4, 6), (7, 17), (3, 1)])
+def test_parallel_io_is_byte_identical_to_printf(tmp_path, threads, prec):
+    """The multithreaded .n parser and writer give the bytes of one strtod and
+    one fprintf("%.*e\\n") per value, for any thread count (values of every
+    magnitude and sign, including zeros and subnormals)."""
+    Nx, Ny = 96, 80
+    rng = np.random.default_rng(threads * 100 + prec)
+    v = rng.normal(size=Nx * Ny) * 10.0 ** rng.integers(-30, 30, size=Nx * Ny)
+    v[:5] = [0.0, -0.0, 5e-324, -2.2250738585072014e-308, 1.7976931348623157e308]
+    # irregular whitespace between values, as fscanf(" %lf") accepts
+    seps = ["\n", " ", "\t", "  \n "]
+    body = "".join("%.17g%s" % (x, seps[i % 4]) for i, x in enumerate(v))
+    big_case(tmp_path, Nx, Ny, prec, body)
+    code, out = run(DRV, tmp_path, env_extra={"PFC_B200_CHECK_ONLY": "2", "OMP_NUM_THREADS": str(threads)})
+    assert code == 0, out
+    parsed = np.array([float(t) for t in body.split()])
+    want = "%d %d %.*f %.*f\n" % (Nx, Ny, prec, 0.785, prec, 0.785) + "".join("%.*e\n" % (prec, x) for x in parsed)
+    assert (tmp_path / "in0.n.check").read_text() == want
+
+
+@pytest.mark.parametrize("threads", [1, 5])
+def test_parallel_parse_errors_follow_the_reference(tmp_path, threads):
+    """A bad token among the first Nx*Ny values is error 38 (the reference's
+    fscanf failure); values and garbage after the first Nx*Ny are never read."""
+    Nx, Ny = 64, 64
+    vals = ["%.12e" % x for x in synth.noise_state(Nx, Ny, 0.25, 0.05, 3).ravel()]
+    env = {"OMP_NUM_THREADS": str(threads)}
+    bad = list(vals)
+    bad[3000] = "x1.0"
+    big_case(tmp_path, Nx, Ny, 6, "\n".join(bad) + "\n")
+    assert run(DRV, tmp_path, env_extra=env)[0] == 38
+    big_case(tmp_path, Nx, Ny, 6, "\n".join(vals[:-1]) + "\n")
+    assert run(DRV, tmp_path, env_extra=env)[0] == 38
+    big_case(tmp_path, Nx, Ny, 6, "\n".join(vals + ["1.0", "junk", "2.0"]) + "\n")
+    assert run(DRV, tmp_path, env_extra=env)[0] == 0
