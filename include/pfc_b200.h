@@ -143,6 +143,13 @@ int pfcg_evaluate(pfcg_handle* h, double* fave, double* nave, double* f);
  * *d is the sampling step (in/out; relax() starts it at 1e-4, :1296). */
 int pfcg_optimize(pfcg_handle* h, int xopt, int yopt, double* d);
 
+/* Field u of the current state smoothed by the model's kernel
+ * G(k) = exp(-k^2 / (2 sigma^2)) (sigma of pfcg_params), written to out (HOST,
+ * Ny*Nx doubles). Replaces the smooth tool (demos/honey/smooth.c:81-121:
+ * r2c, multiply by G, c2r, normalise by the sum of the real-space kernel,
+ * which is exactly 1 since G(0) = 1). */
+int pfcg_smooth(pfcg_handle* h, int u, double* out);
+
 /* Makes `device` the CUDA device that later pfcg_create calls on this host
  * thread use (one process per GPU). No counterpart in the reference, whose
  * ranks are MPI processes (pfc-relax.c:1395-1401). */

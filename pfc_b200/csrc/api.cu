@@ -527,6 +527,34 @@ template <typename T> int eval_sums(pfcg_handle* h, int ntrial, const double* dx
 	return 0;
 }
 
+// Field u convolved with the smoothing kernel G(k) = exp(-k^2 / (2 sigma^2)) of
+// the handle's model, in real space: c2r(G * N_u) plus the FP64 mean (G(0) = 1).
+template <typename T> int do_smooth(pfcg_handle* h, int u, double* out, cudaMemcpyKind kind) {
+	int rc = ensure_real(h);
+	if (rc) return rc;
+	if (!h->work1) CK(h, cudaMalloc(&h->work1, h->celem * (size_t)h->H * h->Ny));
+	CK(h, cudaMemcpyAsync(h->offs, h->mean + u, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+	YArgs<T> ya = yargs<T>(h);
+	ya.work = (cplx<T>*)h->work1;
+	ya.sb = h->sby1;
+	ya.wkind = W_G;
+	ya.wsrc = u;
+	ya.wp = WParams{};
+	rc = run_ypass<T>(h, YP_WEIGHT, ya, h->cy1);
+	if (rc) return rc;
+	XArgs<T> x1 = xargs<T>(h);
+	x1.work = (cplx<T>*)h->work1;
+	x1.m.U = 1;
+	x1.sb = h->sbx1;
+	x1.off = h->offs;
+	x1.real = h->d_real;
+	rc = run_xpass<T>(h, XP_C2R, x1, h->cx1);
+	if (rc) return rc;
+	CK(h, cudaMemcpyAsync(out, h->d_real, sizeof(double) * (size_t)h->Nx * h->Ny, kind, h->stream));
+	CK(h, cudaStreamSynchronize(h->stream));
+	return 0;
+}
+
 template <typename T> int energy_field(pfcg_handle* h, double* f_host) {
 	const long long npts = (long long)h->Nx * h->Ny;
 	const int U = h->U;
@@ -794,6 +822,13 @@ int pfcg_download_device(pfcg_handle* h, double* d_fields) {
 	if (!h || !d_fields) return fail(h, PFCG_EARG, "NULL argument");
 	return h->prec == PFCG_FP64 ? do_download<double>(h, d_fields, cudaMemcpyDeviceToDevice)
 	                            : do_download<float>(h, d_fields, cudaMemcpyDeviceToDevice);
+}
+
+int pfcg_smooth(pfcg_handle* h, int u, double* out) {
+	if (!h || !out) return fail(h, PFCG_EARG, "NULL argument");
+	if (u < 0 || u >= h->U) return fail(h, PFCG_EARG, "field index out of range");
+	return h->prec == PFCG_FP64 ? do_smooth<double>(h, u, out, cudaMemcpyDeviceToHost)
+	                            : do_smooth<float>(h, u, out, cudaMemcpyDeviceToHost);
 }
 
 int pfcg_warmstart(pfcg_handle* h, pfcg_fno* f) {

@@ -760,10 +760,11 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 	constexpr bool REGIO = C::CT && MODE == YP_STEP && !(C::FUSED && FUSEDK) && C::NSUB == C::S &&
 	                       C::S * (NCX / MAXE) == C::NT && PLX::FUSABLE;
 	using RBY = RegBlock<NCX, MAXE, C::S, C::NT, T>;
+	constexpr int CCX = C::CT ? CCC : 1;
 	// global address of element y of resident sequence p (field p / CCC, column p % CCC)
 	auto gaddr = [&](int p, int y) -> long long {
-		return (long long)(p / (C::CT ? CCC : 1)) * a.wstride + (long long)(y / RC) * tileH +
-		       (long long)(kx0 + p % (C::CT ? CCC : 1)) * RC + y % RC;
+		return (long long)(p / CCX) * a.wstride + (long long)(y / R) * tileH + (long long)(kx0 + p % CCX) * R +
+		       y % R;
 	};
 	bool regio = false;
 	if constexpr (REGIO) {
@@ -773,7 +774,7 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 #pragma unroll
 			for (int i = 0; i < RBY::NB; i++) {
 				const int p = RBY::seq(tid, i);
-				const bool live = p % CCC < ncol;
+				const bool live = p % CCX < ncol;
 #pragma unroll
 				for (int r = 0; r < MAXE; r++)
 					rb.v[i][r] = live ? a.work[gaddr(p, RBY::pos(tid, i, r))] : mk<T>((T)0, (T)0);
@@ -961,7 +962,7 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 #pragma unroll
 			for (int i = 0; i < RBY::NB; i++) {
 				const int p = RBY::seq(tid, i);
-				if (p % CCC < ncol) {
+				if (p % CCX < ncol) {
 #pragma unroll
 					for (int r = 0; r < MAXE; r++) a.work[gaddr(p, RBY::pos(tid, i, r))] = rb.v[i][r];
 				}

@@ -45,6 +45,7 @@ SIGNATURES = {
     "pfcg_step": (ctypes.c_int, [_vp, _ip]),
     "pfcg_evaluate": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
     "pfcg_optimize": (ctypes.c_int, [_vp, _ip, _ip, _dp]),
+    "pfcg_smooth": (ctypes.c_int, [_vp, _ip, _dp]),
     "pfcg_set_device": (ctypes.c_int, [_ip]),
     "pfcg_set_profiling": (ctypes.c_int, [_vp, _ip]),
     "pfcg_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _ip]),
@@ -173,6 +174,12 @@ class Relaxation:
     def download_device(self, ptr: int) -> None:
         """Downloads the fields to U*Ny*Nx doubles of DEVICE memory at ptr."""
         self._check(self.L.pfcg_download_device(self.h, ctypes.c_void_p(ptr)))
+
+    def smooth(self, u: int = 0) -> np.ndarray:
+        """Field u smoothed by the model's kernel exp(-k^2 / (2 sigma^2))."""
+        out = np.empty((self.Ny, self.Nx))
+        self._check(self.L.pfcg_smooth(self.h, u, _dptr(out)))
+        return out
 
     def warmstart(self, net) -> None:
         """Replaces the fields by the warm-start network's proposal (U = 2)."""

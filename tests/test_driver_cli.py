@@ -207,3 +207,61 @@ def test_parallel_parse_errors_follow_the_reference(tmp_path, threads):
     assert run(DRV, tmp_path, env_extra=env)[0] == 38
     big_case(tmp_path, Nx, Ny, 6, "\n".join(vals + ["1.0", "junk", "2.0"]) + "\n")
     assert run(DRV, tmp_path, env_extra=env)[0] == 0
+
+
+SMOOTH = os.path.join(ROOT, "pfc_b200", "smooth")
+REF_SMOOTH = os.path.join(ROOT, "oracle", "_ref", "smooth")
+
+
+def test_smooth_usage_and_missing_input(tmp_path):
+    r = subprocess.run([SMOOTH], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "smooth" in r.stdout
+    r = subprocess.run([SMOOTH, "nope.n", "out.n", "0.5"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Input file not found!" in r.stdout
+
+
+def smooth_numpy(f, dx, dy, sigma):
+    """The smoothing of demos/honey/smooth.c:81-121 in numpy: r2c, multiply by
+    exp(-k^2 / (2 sigma^2)), c2r (the kernel's real-space sum is 1)."""
+    H, W = f.shape
+    kx = 2 * np.pi / (dx * W) * np.arange(W // 2 + 1)
+    ky = 2 * np.pi / (dy * H) * np.where(np.arange(H) < H // 2, np.arange(H), np.arange(H) - H)
+    k2 = kx[None, :] ** 2 + ky[:, None] ** 2
+    return np.fft.irfft2(np.fft.rfft2(f) * np.exp(-0.5 / sigma ** 2 * k2), s=f.shape)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-6)])
+def test_smooth_matches_numpy_and_reference(tmp_path, precision, tol):
+    W, H, dx, dy, sigma = 96, 64, 0.7, 0.65, 0.6
+    f = synth.hetero2(W, H, dx, dy, 4, 0, 0, (0.3, -0.3), (0.3, 0.3), (7.2552, 7.5), 0.02, 4)[0]
+    (tmp_path / "in.n").write_text("%d %d %.12f %.12f\n" % (W, H, dx, dy) + "".join("%.17e\n" % v for v in f.ravel()))
+    env = dict(os.environ, PFC_B200_PRECISION=precision)
+    r = subprocess.run([SMOOTH, "in.n", "out.n", str(sigma)], cwd=tmp_path, capture_output=True, text=True,
+                       env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    lines = (tmp_path / "out.n").read_text().splitlines()
+    assert lines[0] == "%d %d %f %f" % (W, H, dx, dy)
+    assert all(len(l.split("e")[0].split(".")[1]) == 12 for l in lines[1:])
+    got = np.array([float(x) for x in lines[1:]]).reshape(H, W)
+    want = smooth_numpy(f, dx, dy, sigma)
+    assert np.abs(got - want).max() < tol * np.abs(want).max()
+    if os.path.exists(REF_SMOOTH):
+        r = subprocess.run([REF_SMOOTH, "in.n", "ref.n", str(sigma)], cwd=tmp_path, capture_output=True, timeout=120)
+        assert r.returncode == 0
+        ref = np.loadtxt(tmp_path / "ref.n", skiprows=1).reshape(H, W)
+        assert np.abs(got - ref).max() < tol * np.abs(ref).max()
+
+
+def test_numpy_smoothing_matches_reference_binary(tmp_path):
+    """Pins smooth_numpy (the GPU test's oracle) to the reference smooth tool
+    built from its own source over the FFT shim (CPU)."""
+    if not os.path.exists(REF_SMOOTH):
+        pytest.skip("reference smooth not built")
+    W, H, dx, dy, sigma = 48, 40, 0.7, 0.65, 0.6
+    f = synth.noise_state(W, H, 0.1, 0.3, 12)
+    (tmp_path / "in.n").write_text("%d %d %.12f %.12f\n" % (W, H, dx, dy) + "".join("%.17e\n" % v for v in f.ravel()))
+    r = subprocess.run([REF_SMOOTH, "in.n", "ref.n", str(sigma)], cwd=tmp_path, capture_output=True, timeout=120)
+    assert r.returncode == 0
+    ref = np.loadtxt(tmp_path / "ref.n", skiprows=1).reshape(H, W)
+    assert np.abs(smooth_numpy(f, dx, dy, sigma) - ref).max() < 1e-12 * np.abs(ref).max()
