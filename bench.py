@@ -52,6 +52,23 @@ def workload(N: int, rank: int):
     return pd, dx, dy, f
 
 
+def reduce_max(x: float, dist=None, device="cpu") -> float:
+    """Max of x over the ranks of the process group (x itself without one)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(steps: int, seconds_max: float, world: int) -> float:
+    """Whole-job steps/s of `world` independent replicas that each took `steps`
+    steps, timed as the slowest rank (weak scaling)."""
+    return steps * world / seconds_max
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as fh:
@@ -396,11 +413,7 @@ def main():
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = reduce_max(e0.elapsed_time(e1), dist, "cuda")
         return ms, r.launches - l0
 
     results = {}
@@ -423,7 +436,7 @@ def main():
     main_p = args.precision
     res = results[main_p]
     ms = res["ms"]
-    steps_per_s = args.steps * 1000.0 / ms * world
+    steps_per_s = aggregate_rate(args.steps, ms * 1e-3, world)
     eb = 4 if main_p == "fp32" else 8
     # algorithmic bytes (complex elements of 2*eb bytes): y-pass reads work and
     # spec, writes spec and work (4 per point); x-pass reads and writes work (2)
@@ -454,12 +467,8 @@ def main():
     r.evaluate()
     r.download(hout)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": args.steps / e2e_s * world, "unit": "steps/s",
+    e2e_s = reduce_max(time.perf_counter() - t0, dist, "cuda")
+    e2e = {"value": aggregate_rate(args.steps, e2e_s, world), "unit": "steps/s",
            "h2d_bytes_per_step": int(hin.nbytes / args.steps),
            "d2h_bytes_per_step": int((hout.nbytes + 8 * (1 + U)) / args.steps),
            "note": "one relaxation call sequence per run: upload, %d steps, evaluate, download" % args.steps}
