@@ -150,6 +150,20 @@ int pfcg_optimize(pfcg_handle* h, int xopt, int yopt, double* d);
  * which is exactly 1 since G(0) = 1). */
 int pfcg_smooth(pfcg_handle* h, int u, double* out);
 
+/* Orientation and deformation fields of a density field (Nx*Ny doubles, HOST),
+ * replacing the fields tool (src/fields.c): psi (HOST, 2*Ny*Nx doubles: the
+ * real plane, then the imaginary plane) is the complex orientation field,
+ * (density - min) convolved with exp(-(|k|-1)^2 / (2 sk^2)) exp(i fold
+ * atan2(ky, kx)), times (density - min), smoothed by exp(-k^2 / (2 sb^2)) and
+ * normalised to max |psi| = 1 (fields.c:103-200); chi (HOST, Ny*Nx, or NULL to
+ * skip it) is the deformation field, the sum over Gaussian scales 1/2, 1/4, ...
+ * (while 4 pi/sqrt(3) times the scale index stays below half the box) of the
+ * maximum-normalised smoothing of |grad psi_unnormalised|^power
+ * (fields.c:218-320). fold must be even (the reference's method works only
+ * for even folds). Transforms in FP64. Uses the current device. */
+int pfcg_fields(const double* density, int Nx, int Ny, double dx, double dy, int fold, double sk, double sb,
+                double power, double* psi, double* chi);
+
 /* Makes `device` the CUDA device that later pfcg_create calls on this host
  * thread use (one process per GPU). No counterpart in the reference, whose
  * ranks are MPI processes (pfc-relax.c:1395-1401). */

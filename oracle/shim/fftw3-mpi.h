@@ -62,6 +62,10 @@ ptrdiff_t fftw_mpi_local_size_2d_transposed(ptrdiff_t n0, ptrdiff_t n1, MPI_Comm
 ptrdiff_t fftw_mpi_local_size_2d(ptrdiff_t n0, ptrdiff_t n1, MPI_Comm comm, ptrdiff_t* local_n0, ptrdiff_t* local_0_start);
 fftw_plan fftw_mpi_plan_dft_r2c_2d(ptrdiff_t n0, ptrdiff_t n1, double* in, fftw_complex* out, MPI_Comm comm, unsigned flags);
 fftw_plan fftw_mpi_plan_dft_c2r_2d(ptrdiff_t n0, ptrdiff_t n1, fftw_complex* in, double* out, MPI_Comm comm, unsigned flags);
+/* complex 2-D transform; FFTW_MPI_TRANSPOSED_OUT (forward) leaves [n1][n0],
+ * FFTW_MPI_TRANSPOSED_IN (backward) takes [n1][n0]; unnormalised */
+fftw_plan fftw_mpi_plan_dft_2d(ptrdiff_t n0, ptrdiff_t n1, fftw_complex* in, fftw_complex* out, MPI_Comm comm, int sign,
+                               unsigned flags);
 void fftw_execute(const fftw_plan p);
 void fftw_destroy_plan(fftw_plan p);
 void* fftw_malloc(size_t n);

@@ -555,6 +555,37 @@ template <typename T> int do_smooth(pfcg_handle* h, int u, double* out, cudaMemc
 	return 0;
 }
 
+// out = c2r(w(k) * spectrum) + offset for one weight of YP_WEIGHT (device out, Ny*Nx)
+template <typename T> int weighted_c2r(pfcg_handle* h, int kind, int src, const WParams& wp, double offset, double* out) {
+	if (!h->work1) CK(h, cudaMalloc(&h->work1, h->celem * (size_t)h->H * h->Ny));
+	CK(h, cudaStreamSynchronize(h->stream)); // the pinned offset slot is free again
+	double* ho = h->h_buf + ACC_N + MAXU;
+	ho[0] = offset;
+	CK(h, cudaMemcpyAsync(h->offs, ho, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+	YArgs<T> ya = yargs<T>(h);
+	ya.work = (cplx<T>*)h->work1;
+	ya.sb = h->sby1;
+	ya.wkind = kind;
+	ya.wsrc = src;
+	ya.wp = wp;
+	int rc = run_ypass<T>(h, YP_WEIGHT, ya, h->cy1);
+	if (rc) return rc;
+	XArgs<T> x1 = xargs<T>(h);
+	x1.work = (cplx<T>*)h->work1;
+	x1.m.U = 1;
+	x1.sb = h->sbx1;
+	x1.off = h->offs;
+	x1.real = out;
+	return run_xpass<T>(h, XP_C2R, x1, h->cx1);
+}
+
+// the FP64 means of the current state, on the host
+int host_means(pfcg_handle* h, double* m) {
+	CK(h, cudaMemcpyAsync(m, h->mean, sizeof(double) * h->U, cudaMemcpyDeviceToHost, h->stream));
+	CK(h, cudaStreamSynchronize(h->stream));
+	return 0;
+}
+
 template <typename T> int energy_field(pfcg_handle* h, double* f_host) {
 	const long long npts = (long long)h->Nx * h->Ny;
 	const int U = h->U;
@@ -822,6 +853,136 @@ int pfcg_download_device(pfcg_handle* h, double* d_fields) {
 	if (!h || !d_fields) return fail(h, PFCG_EARG, "NULL argument");
 	return h->prec == PFCG_FP64 ? do_download<double>(h, d_fields, cudaMemcpyDeviceToDevice)
 	                            : do_download<float>(h, d_fields, cudaMemcpyDeviceToDevice);
+}
+
+// fields.c (write_phi :103-216, write_chi :218-343) on a two-field handle whose
+// fields are the real and imaginary parts of the complex field z
+static int fields_impl(pfcg_handle* h, const double* density, int fold, double sk, double sb, double power, double* psi,
+                       double* chi) {
+	const long long n = (long long)h->Nx * h->Ny;
+	std::vector<double> host(2 * n, 0.0);
+	double mn = density[0];
+	for (long long i = 1; i < n; i++) mn = density[i] < mn ? density[i] : mn;
+	for (long long i = 0; i < n; i++) host[i] = density[i] - mn;
+	double *d_s = nullptr, *d_g = nullptr, *d_part = nullptr;
+	auto cleanup = [&]() {
+		cudaFree(d_s);
+		cudaFree(d_g);
+		cudaFree(d_part);
+	};
+	constexpr int NPART = 296;
+	int rc = 0;
+	double m[2];
+	WParams wp{};
+	do {
+		if (cudaMalloc(&d_s, sizeof(double) * n) != cudaSuccess || cudaMalloc(&d_g, sizeof(double) * 4 * n) != cudaSuccess ||
+		    cudaMalloc(&d_part, sizeof(double) * NPART) != cudaSuccess) {
+			rc = fail(h, PFCG_ENOMEM, "fields: device allocation failed");
+			break;
+		}
+		if (cudaMemcpy(d_s, host.data(), sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+			rc = fail(h, PFCG_ECUDA, "fields: copy failed");
+			break;
+		}
+		// z = (density - min) convolved with the complex orientation kernel
+		if ((rc = do_upload<double>(h, host.data(), cudaMemcpyHostToDevice))) break;
+		if ((rc = host_means(h, m))) break;
+		const double k0 = std::exp(-0.5 / (sk * sk)); // the kernel at k = 0
+		wp.sk = sk;
+		wp.fold = fold;
+		wp.part = 0;
+		if ((rc = weighted_c2r<double>(h, W_OR, 0, wp, k0 * m[0], h->d_real))) break;
+		wp.part = 1;
+		if ((rc = weighted_c2r<double>(h, W_OR, 0, wp, k0 * m[1], h->d_real + n))) break;
+		// times (density - min), then Gaussian smoothing with spread sb
+		if (launch_fields_mul(h->d_real, h->d_real + n, d_s, n, h->stream) != cudaSuccess) {
+			rc = fail(h, PFCG_ECUDA, "fields: kernel launch failed");
+			break;
+		}
+		h->launches++;
+		if ((rc = spectral_from_real<double>(h))) break;
+		if ((rc = host_means(h, m))) break;
+		wp = WParams{};
+		wp.gs = sb;
+		if ((rc = weighted_c2r<double>(h, W_GS, 0, wp, m[0], d_g))) break;
+		if ((rc = weighted_c2r<double>(h, W_GS, 1, wp, m[1], d_g + n))) break;
+		if (cudaMemcpyAsync(psi, d_g, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+		    cudaStreamSynchronize(h->stream) != cudaSuccess) {
+			rc = fail(h, PFCG_ECUDA, "fields: copy failed");
+			break;
+		}
+		double mx = 0.0;
+		for (long long i = 0; i < n; i++) mx = std::max(mx, std::hypot(psi[i], psi[n + i]));
+		const double inv = 1.0 / mx;
+		for (long long i = 0; i < 2 * n; i++) psi[i] *= inv;
+		if (!chi) break;
+		// deformation: |grad z|^power of the smoothed z, summed over Gaussian scales 1/2, 1/4, ...
+		for (int k = 0; k < 4; k++) {
+			wp = WParams{};
+			wp.gs = sb;
+			wp.dir = k / 2;
+			if ((rc = weighted_c2r<double>(h, W_DG, k % 2, wp, 0.0, d_g + k * n))) break;
+		}
+		if (rc) break;
+		if (launch_fields_gradpow(d_g, n, power, h->d_real, h->stream) != cudaSuccess ||
+		    cudaMemsetAsync(h->d_real + n, 0, sizeof(double) * n, h->stream) != cudaSuccess) {
+			rc = fail(h, PFCG_ECUDA, "fields: kernel launch failed");
+			break;
+		}
+		h->launches++;
+		if ((rc = spectral_from_real<double>(h))) break;
+		if ((rc = host_means(h, m))) break;
+		double* acc = d_g + n;
+		if (cudaMemsetAsync(acc, 0, sizeof(double) * n, h->stream) != cudaSuccess) {
+			rc = fail(h, PFCG_ECUDA, "fields: memset failed");
+			break;
+		}
+		const double l0 = 4.0 * PI / std::sqrt(3.0);
+		const double L = std::min(h->Nx * h->geom.dx, h->Ny * h->geom.dy);
+		for (int sc = 2; l0 * sc < 0.5 * L; sc *= 2) {
+			wp = WParams{};
+			wp.gs = 1.0 / sc;
+			if ((rc = weighted_c2r<double>(h, W_GS, 0, wp, m[0], d_g))) break;
+			if (launch_scaled_acc(acc, d_g, n, d_part, NPART, h->stream) != cudaSuccess) {
+				rc = fail(h, PFCG_ECUDA, "fields: kernel launch failed");
+				break;
+			}
+			h->launches += 2;
+		}
+		if (rc) break;
+		if (cudaMemcpyAsync(chi, acc, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+		    cudaStreamSynchronize(h->stream) != cudaSuccess)
+			rc = fail(h, PFCG_ECUDA, "fields: copy failed");
+	} while (0);
+	cleanup();
+	return rc;
+}
+
+int pfcg_fields(const double* density, int Nx, int Ny, double dx, double dy, int fold, double sk, double sb,
+                double power, double* psi, double* chi) {
+	if (!density || !psi) return fail(nullptr, PFCG_EARG, "NULL argument");
+	if (fold <= 0 || fold % 2) return fail(nullptr, PFCG_EARG, "the orientation kernel needs an even, positive fold");
+	if (!(sk > 0) || !(sb > 0)) return fail(nullptr, PFCG_EARG, "kernel spreads must be positive");
+	pfcg_params p;
+	std::memset(&p, 0, sizeof(p));
+	p.U = 2;
+	p.c = 1.0;
+	p.dt = 1.0;
+	p.sigma = 1.0;
+	for (int u = 0; u < 2; u++) {
+		p.W[u] = 1;
+		p.alpha[u][u] = -0.25;
+		p.beta[u][u] = 1.0;
+		p.nu2[u][0] = 1.0;
+		p.omega[u][0] = 1.0;
+	}
+	pfcg_handle* h = nullptr;
+	int rc = pfcg_create(&p, Nx, Ny, dx, dy, PFCG_FP64, &h);
+	if (rc) return rc;
+	rc = fields_impl(h, density, fold, sk, sb, power, psi, chi);
+	if (rc) g_err = h->err;
+	pfcg_destroy(h);
+	return rc;
 }
 
 int pfcg_smooth(pfcg_handle* h, int u, double* out) {

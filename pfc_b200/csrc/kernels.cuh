@@ -54,7 +54,11 @@ struct Geom {
 
 enum XMode { XP_STEP = 0, XP_EVAL = 1, XP_C2R = 2, XP_R2C = 3 };
 enum YMode { YP_STEP = 0, YP_INIT = 1, YP_WEIGHT = 2 };
-enum WKind { W_ONE = 0, W_P = 1, W_G = 2, W_Q = 3 };
+// k-space weights of YP_WEIGHT: P_u(k), the model's G(k), (mu2 - k^2)^2, and
+// for the orientation / deformation fields a Gaussian of runtime spread
+// (W_GS), one part of the complex orientation kernel applied to the field pair
+// (W_OR) and a Gaussian-smoothed derivative (W_DG)
+enum WKind { W_ONE = 0, W_P = 1, W_G = 2, W_Q = 3, W_GS = 4, W_OR = 5, W_DG = 6 };
 
 template <typename T> struct XArgs {
 	cplx<T>* work;          // U arrays at stride wstride
@@ -77,6 +81,11 @@ struct WParams {
 	int W;
 	double nu2[MAXW], omega[MAXW], phi[MAXW];
 	double mu2;
+	double gs;   // W_GS, W_DG: Gaussian exp(-k^2 / (2 gs^2))
+	double sk;   // W_OR: radial spread of the kernel exp(-(|k| - 1)^2 / (2 sk^2))
+	int fold;    // W_OR: angular order, exp(i fold atan2(ky, kx)) (even)
+	int part;    // W_OR: 0 -> Kr s0 - Ki s1, 1 -> Ki s0 + Kr s1 (s0, s1 the two fields)
+	int dir;     // W_DG: 0 -> i kx, 1 -> i ky
 };
 
 template <typename T> struct YArgs {
@@ -139,6 +148,13 @@ cudaError_t launch_field_means(const double* real, int U, long long npts, double
 // smoothing couplings from the precomputed real fields (see kernels.cu).
 cudaError_t launch_energy_density(const double* m, const double* pn, const double* eta, const double* q, int npair,
                                   const Model& mod, long long npts, double* f, cudaStream_t s);
+
+// orientation / deformation fields: a *= s and b *= s; out = (sum of the
+// squares of the four fields of g4)^(power/2); acc += r / max(r) (part: nparts
+// doubles of scratch)
+cudaError_t launch_fields_mul(double* a, double* b, const double* s, long long n, cudaStream_t st);
+cudaError_t launch_fields_gradpow(const double* g4, long long n, double power, double* out, cudaStream_t st);
+cudaError_t launch_scaled_acc(double* acc, const double* r, long long n, double* part, int nparts, cudaStream_t st);
 
 int max_elems_per_thread(bool fp64);
 int max_radix(bool fp64);

@@ -126,3 +126,71 @@ cudaError_t launch_field_means(const double* real, int U, long long npts, double
 }
 
 } // namespace pfcg
+
+// ------------------------------------------------- orientation / deformation --
+namespace pfcg {
+namespace {
+__global__ void fields_mul_kernel(double* __restrict__ a, double* __restrict__ b, const double* __restrict__ s,
+                                  long long n) {
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+		a[i] *= s[i];
+		b[i] *= s[i];
+	}
+}
+
+__global__ void fields_gradpow_kernel(const double* __restrict__ g, long long n, double power, double* __restrict__ out) {
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+		const double u2 = g[i] * g[i] + g[n + i] * g[n + i], v2 = g[2 * n + i] * g[2 * n + i] + g[3 * n + i] * g[3 * n + i];
+		out[i] = pow(u2 + v2, 0.5 * power);
+	}
+}
+
+// per-block maxima, then one block takes the maximum of those in a fixed order
+__global__ void max_partials_kernel(const double* __restrict__ x, long long n, double* __restrict__ part) {
+	__shared__ double red[32];
+	double m = -INFINITY;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		m = fmax(m, x[i]);
+	for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+	__syncthreads();
+	if (threadIdx.x < 32) {
+		m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : -INFINITY;
+		for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+		if (threadIdx.x == 0) part[blockIdx.x] = m;
+	}
+}
+
+// acc += r / max(r), the maximum taken from the partials
+__global__ void scaled_acc_kernel(double* __restrict__ acc, const double* __restrict__ r, const double* __restrict__ part,
+                                  int nparts, long long n) {
+	__shared__ double m;
+	if (threadIdx.x == 0) {
+		double v = -INFINITY;
+		for (int k = 0; k < nparts; k++) v = fmax(v, part[k]);
+		m = v;
+	}
+	__syncthreads();
+	const double inv = 1.0 / m;
+	for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		acc[i] += r[i] * inv;
+}
+
+int grid_of(long long n) { return (int)((n + 255) / 256 > 148 * 8 ? 148 * 8 : (n + 255) / 256); }
+} // namespace
+
+cudaError_t launch_fields_mul(double* a, double* b, const double* s, long long n, cudaStream_t st) {
+	fields_mul_kernel<<<grid_of(n), 256, 0, st>>>(a, b, s, n);
+	return cudaGetLastError();
+}
+cudaError_t launch_fields_gradpow(const double* g4, long long n, double power, double* out, cudaStream_t st) {
+	fields_gradpow_kernel<<<grid_of(n), 256, 0, st>>>(g4, n, power, out);
+	return cudaGetLastError();
+}
+cudaError_t launch_scaled_acc(double* acc, const double* r, long long n, double* part, int nparts, cudaStream_t st) {
+	max_partials_kernel<<<nparts, 256, 0, st>>>(r, n, part);
+	scaled_acc_kernel<<<grid_of(n), 256, 0, st>>>(acc, r, part, nparts, n);
+	return cudaGetLastError();
+}
+
+} // namespace pfcg

@@ -929,8 +929,32 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp) {
 				} else if (a.wkind == W_Q) {
 					const double d = a.wp.mu2 - k2;
 					w = d * d;
+				} else if (a.wkind == W_GS || a.wkind == W_DG) {
+					w = exp(-0.5 * k2 / (a.wp.gs * a.wp.gs));
 				}
-				nn = cscale(src[(long long)kx * Ny + ky], (T)w);
+				const long long si = (long long)kx * Ny + ky;
+				if (a.wkind == W_OR) {
+					// orientation kernel K = exp(-(|k| - 1)^2 / (2 sk^2)) exp(i fold phi),
+					// fields.c:143-153; real and imaginary parts are even in k
+					// for even fold, so each part maps the field pair to a real field
+					const double kxv = kx * a.g.dkx;
+					const double kyv = (ky < Ny / 2 ? ky : ky - Ny) * a.g.dky;
+					const double q = sqrt(k2) - 1.0;
+					const double rad = exp(-0.5 * q * q / (a.wp.sk * a.wp.sk));
+					double sn, cs;
+					sincos(a.wp.fold * atan2(kyv, kxv), &sn, &cs);
+					const T kr = (T)(rad * cs), ki = (T)(rad * sn);
+					const cplx<T> s0 = a.spec[si], s1 = a.spec[a.sstride + si];
+					nn = a.wp.part == 0 ? csub(cscale(s0, kr), cscale(s1, ki)) : cadd(cscale(s0, ki), cscale(s1, kr));
+				} else if (a.wkind == W_DG) {
+					// i k_dir G(k) times the field (fields.c:260-271 on the smoothed spectrum)
+					const double kd = a.wp.dir == 0 ? kx * a.g.dkx : (ky < Ny / 2 ? ky : ky - Ny) * a.g.dky;
+					const cplx<T> v = src[si];
+					const T f = (T)(kd * w);
+					nn = mk<T>(-f * v.y, f * v.x);
+				} else {
+					nn = cscale(src[si], (T)w);
+				}
 			}
 			sm[c * ld + pad<T>(ky)] = nn;
 		}

@@ -72,15 +72,14 @@ int nio_parse_values(const char* q, const char* e, double* out, size_t n) {
 	return fail;
 }
 
-void nio_write_values(FILE* f, int prec, const double* v, size_t n) {
-	/* blocks of B values are formatted in parallel, one buffer each, then
-	 * written in order */
+/* blocks of B lines are formatted in parallel, one buffer each, then written in order */
+static void write_blocks(FILE* f, int prec, const double* a, const double* b, size_t n) {
 	int nt = 1;
 #ifdef _OPENMP
 	nt = omp_get_max_threads();
 #endif
 	const size_t B = 1 << 15;
-	const size_t per = 48 + (size_t)(prec > 0 ? prec : 0); /* "-d." + digits + "e+ddd\n" and margin */
+	const size_t per = (b ? 2 : 1) * (48 + (size_t)(prec > 0 ? prec : 0));
 	char** buf = (char**)malloc(sizeof(char*) * nt);
 	size_t* used = (size_t*)malloc(sizeof(size_t) * nt);
 	for (int k = 0; k < nt; k++) buf[k] = (char*)malloc(B * per);
@@ -90,7 +89,9 @@ void nio_write_values(FILE* f, int prec, const double* v, size_t n) {
 			const size_t i0 = g0 + (size_t)k * B;
 			const size_t i1 = i0 + B < n ? i0 + B : n;
 			size_t pos = 0;
-			for (size_t i = i0; i < i1; i++) pos += (size_t)snprintf(buf[k] + pos, per, "%.*e\n", prec, v[i]);
+			for (size_t i = i0; i < i1; i++)
+				pos += b ? (size_t)snprintf(buf[k] + pos, per, "%.*e %.*e\n", prec, a[i], prec, b[i])
+				         : (size_t)snprintf(buf[k] + pos, per, "%.*e\n", prec, a[i]);
 			used[k] = i0 < n ? pos : 0;
 		}
 		for (int k = 0; k < nt; k++)
@@ -100,6 +101,10 @@ void nio_write_values(FILE* f, int prec, const double* v, size_t n) {
 	free(buf);
 	free(used);
 }
+
+void nio_write_pairs(FILE* f, int prec, const double* a, const double* b, size_t n) { write_blocks(f, prec, a, b, n); }
+
+void nio_write_values(FILE* f, int prec, const double* v, size_t n) { write_blocks(f, prec, v, NULL, n); }
 
 char* nio_slurp(const char* path, size_t* len) {
 	FILE* f = fopen(path, "rb");

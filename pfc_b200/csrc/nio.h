@@ -15,6 +15,9 @@ int nio_parse_values(const char* q, const char* e, double* out, size_t n);
 /* fprintf(f, "%.*e\n", prec, v[i]) for i = 0 .. n-1. */
 void nio_write_values(FILE* f, int prec, const double* v, size_t n);
 
+/* fprintf(f, "%.*e %.*e\n", prec, a[i], prec, b[i]) for i = 0 .. n-1. */
+void nio_write_pairs(FILE* f, int prec, const double* a, const double* b, size_t n);
+
 /* Whole file into a NUL-terminated buffer (free() it); NULL if unreadable. */
 char* nio_slurp(const char* path, size_t* len);
 

@@ -46,6 +46,8 @@ SIGNATURES = {
     "pfcg_evaluate": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
     "pfcg_optimize": (ctypes.c_int, [_vp, _ip, _ip, _dp]),
     "pfcg_smooth": (ctypes.c_int, [_vp, _ip, _dp]),
+    "pfcg_fields": (ctypes.c_int, [_dp, _ip, _ip, ctypes.c_double, ctypes.c_double, _ip, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, _dp, _dp]),
     "pfcg_set_device": (ctypes.c_int, [_ip]),
     "pfcg_set_profiling": (ctypes.c_int, [_vp, _ip]),
     "pfcg_profile_read": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_longlong), _ip]),
@@ -323,6 +325,20 @@ def init_hetero(d_fields_ptr: int, Nx: int, Ny: int, dx: float, dy: float, spec:
     rc = L.pfcg_init_hetero(ctypes.c_void_p(d_fields_ptr), Nx, Ny, dx, dy, ctypes.byref(spec), ctypes.c_void_p(stream))
     if rc:
         raise PfcError(rc, L.pfcg_init_last_error().decode())
+
+
+def fields(density: np.ndarray, dx: float, dy: float, fold: int, sk: float, sb: float, power: float | None = None):
+    """pfcg_fields: (psi complex (Ny, Nx), chi (Ny, Nx) or None)."""
+    L = load()
+    d = np.ascontiguousarray(density, dtype=np.float64)
+    Ny, Nx = d.shape
+    psi = np.empty((2, Ny, Nx))
+    chi = np.empty((Ny, Nx)) if power is not None else None
+    rc = L.pfcg_fields(_dptr(d), Nx, Ny, dx, dy, fold, sk, sb, power or 0.0, _dptr(psi),
+                       _dptr(chi) if chi is not None else None)
+    if rc:
+        raise PfcError(rc, L.pfcg_last_error(None).decode())
+    return psi[0] + 1j * psi[1], chi
 
 
 def last_error() -> str:

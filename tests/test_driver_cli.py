@@ -265,3 +265,81 @@ def test_numpy_smoothing_matches_reference_binary(tmp_path):
     assert r.returncode == 0
     ref = np.loadtxt(tmp_path / "ref.n", skiprows=1).reshape(H, W)
     assert np.abs(smooth_numpy(f, dx, dy, sigma) - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+FIELDS = os.path.join(ROOT, "pfc_b200", "fields")
+REF_FIELDS = os.path.join(ROOT, "oracle", "_ref", "fields")
+
+
+def polycrystal_file(path, W=128, H=96, seed=3):
+    dx = dy = synth.A_TRI / 8
+    p = synth.polycrystal(W, H, dx, dy, 5, 0.0, 0.5, 0.02, seed)
+    path.write_text("%d %d %.12f %.12f\n" % (W, H, dx, dy) + "".join("%.17e\n" % v for v in p.ravel()))
+    return p, dx, dy
+
+
+@pytest.mark.parametrize("args,code,msg", [((), 0, "fields"), (("a", "b"), 1, "Error: Invalid syntax."),
+                                           (("nope.n", "o.phi", "6", "0.2", "0.1"), 1, "Error: Input file not found.")])
+def test_fields_cli_messages(tmp_path, args, code, msg):
+    r = subprocess.run([FIELDS] + list(args), cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == code and msg in r.stdout
+    if os.path.exists(REF_FIELDS) and args:
+        rr = subprocess.run([REF_FIELDS] + list(args), cwd=tmp_path, capture_output=True, text=True, timeout=60)
+        assert rr.returncode == code and msg in rr.stdout
+
+
+def test_fields_oracle_matches_reference_binary(tmp_path):
+    """Pins oracle/fields_oracle.py (the GPU test's checker) to the reference
+    tool compiled over the FFT shim, to the reference's print precision."""
+    if not os.path.exists(REF_FIELDS):
+        pytest.skip("reference fields not built")
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fields_oracle as FO
+
+    p, dx, dy = polycrystal_file(tmp_path / "d.n")
+    r = subprocess.run([REF_FIELDS, "d.n", "o.phi", "o.chi", "6", "0.2", "0.1", "2.0"], cwd=tmp_path,
+                       capture_output=True, timeout=120)
+    assert r.returncode == 0
+    ref = np.loadtxt(tmp_path / "o.phi", skiprows=1)
+    refc = np.loadtxt(tmp_path / "o.chi", skiprows=1)
+    psi, Z = FO.orientation(p, dx, dy, 6, 0.2, 0.1)
+    chi = FO.deformation(Z, dx, dy, 2.0)
+    # "%e" keeps 7 significant digits
+    assert np.abs(ref[:, 0] - psi.real.ravel()).max() < 6e-7
+    assert np.abs(ref[:, 1] - psi.imag.ravel()).max() < 6e-7
+    assert np.abs(refc - chi.ravel()).max() < 6e-7 * np.abs(chi).max()
+
+
+@pytest.mark.gpu
+def test_fields_gpu_matches_oracle_and_reference(tmp_path):
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fields_oracle as FO
+
+    p, dx, dy = polycrystal_file(tmp_path / "d.n")
+    psi, chi = lib.fields(p, dx, dy, 6, 0.2, 0.1, 2.0)
+    want_psi, Z = FO.orientation(p, dx, dy, 6, 0.2, 0.1)
+    want_chi = FO.deformation(Z, dx, dy, 2.0)
+    assert np.abs(psi - want_psi).max() < 1e-9
+    assert np.abs(chi - want_chi).max() < 1e-9 * np.abs(want_chi).max()
+    # the command-line tool writes the reference's format
+    r = subprocess.run([FIELDS, "d.n", "o.phi", "o.chi", "6", "0.2", "0.1", "2.0"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    got = np.loadtxt(tmp_path / "o.phi", skiprows=1)
+    assert np.abs(got[:, 0] - want_psi.real.ravel()).max() < 6e-7
+    if os.path.exists(REF_FIELDS):
+        subprocess.run([REF_FIELDS, "d.n", "r.phi", "r.chi", "6", "0.2", "0.1", "2.0"], cwd=tmp_path, timeout=120)
+        assert (tmp_path / "o.phi").read_text().splitlines()[0] == (tmp_path / "r.phi").read_text().splitlines()[0]
+        ref = np.loadtxt(tmp_path / "r.phi", skiprows=1)
+        assert np.abs(got - ref).max() < 1.2e-6
+        assert np.abs(np.loadtxt(tmp_path / "o.chi", skiprows=1) - np.loadtxt(tmp_path / "r.chi", skiprows=1)).max() \
+            < 1.2e-6 * np.abs(want_chi).max()
+
+
+@pytest.mark.gpu
+def test_fields_rejects_odd_fold():
+    p = synth.noise_state(32, 32, 0.0, 0.1, 1)
+    with pytest.raises(lib.PfcError):
+        lib.fields(p, 0.9, 0.9, 3, 0.2, 0.1)
