@@ -286,7 +286,7 @@ def run_ttr(args):
     free energy changes by less than 1e-9 per step over a 100-step window,
     with the wall time of the whole run (every step and evaluation, and for the
     warm start the network's tiled application). Three arms from the same
-    initial state: the plain FP64 iteration (the judge), the plain FP32
+    initial state: the plain FP64 iteration (the reference precision), the plain FP32
     iteration, and FP32 with the learned warm start (the network's input step of
     plain steps, the network, then the plain finish). Creating the network and
     loading its weights is reported apart, as set-up."""

@@ -89,7 +89,7 @@ int main(int argc, char** argv) {
 		return 1;
 	}
 	if (!pfcg_size_supported((int)W, (int)H)) {
-		fprintf(stderr, "grid size not supported by this build (need even sizes 8..8192 with prime factors 2, 3, 5, 7).\n");
+		fprintf(stderr, "grid size not supported by pfc_b200 (need even sizes 8..8192 with prime factors 2, 3, 5, 7).\n");
 		return 42;
 	}
 	double* psi = (double*)malloc(sizeof(double) * 2 * n);

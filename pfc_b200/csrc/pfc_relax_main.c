@@ -79,7 +79,7 @@ static const char* const MESSAGES[] = {
 	"Error: Invalid syntax.",
 };
 
-/* codes beyond the reference's: limits of this build and device errors */
+/* codes beyond the reference's: limits of pfc_b200 and device errors */
 #define E_UNSUPPORTED 42
 #define E_DEVICE 43
 
@@ -160,7 +160,7 @@ static void parse_I(FILE* in, Config* s) {
 	read_line(in, line);
 	const int prevU = s->U;
 	s->U += count_words(line);
-	if (s->U > PFCG_MAX_U) die_msg(E_UNSUPPORTED, "more than 4 density fields are not supported by this build.");
+	if (s->U > PFCG_MAX_U) die_msg(E_UNSUPPORTED, "more than 4 density fields are not supported by pfc_b200.");
 	q = line;
 	s->Nx = s->Ny = -1;
 	for (int u = 0; u < s->U; u++) {
@@ -262,7 +262,7 @@ static void parse_M(FILE* in, Config* s) {
 	for (int u = 0; u < U; u++) {
 		read_line(in, line);
 		const int W = count_words(line);
-		if (W > PFCG_MAX_W) die_msg(E_UNSUPPORTED, "more than 4 modes per density field are not supported by this build.");
+		if (W > PFCG_MAX_W) die_msg(E_UNSUPPORTED, "more than 4 modes per density field are not supported by pfc_b200.");
 		p->W[u] = W;
 		const char* q = line;
 		for (int w = 0; w < W; w++) {
@@ -459,7 +459,7 @@ int main(int argc, char** argv) {
 		return 0;
 	}
 	if (!pfcg_size_supported(s.Nx, s.Ny))
-		die_msg(E_UNSUPPORTED, "grid size not supported by this build (need even sizes 8..8192 with prime factors 2, 3, 5, 7).");
+		die_msg(E_UNSUPPORTED, "grid size not supported by pfc_b200 (need even sizes 8..8192 with prime factors 2, 3, 5, 7).");
 
 	const char* pe = getenv("PFC_B200_PRECISION");
 	const pfcg_prec prec = (pe && strcmp(pe, "fp32") == 0) ? PFCG_FP32 : PFCG_FP64;

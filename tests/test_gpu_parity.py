@@ -5,7 +5,7 @@ Tolerances: the FP64 path follows the reference's arithmetic except for the
 FFT (own Stockham on the GPU) and the Parseval form of the energy, so it agrees
 to rounding amplified by the dynamics (fields 1e-9 absolute, energies 1e-9
 relative; the box optimisation amplifies energy rounding into dx, dy at the
-1e-10 level). The FP32 path is held to the north-star bound: relative
+1e-10 level). The FP32 path is held to the FP32 accuracy bound: relative
 difference of <f> against FP64 of at most 1e-6 while the field is near a
 relaxed state, with max |dpsi| stated.
 """
@@ -80,7 +80,7 @@ def test_golden_fp32(name):
 @pytest.mark.parametrize("name", golden_names())
 def test_fp32_near_relaxed_energy_bound(name):
     """From the reference's final (near-relaxed) state, FP32 and FP64 GPU runs
-    of 200 more steps agree on <f> to 1e-6 relative and
+    of 200 more steps agree on <f> to 1e-6 relative (the FP32 accuracy bound) and
     on the field to max |dpsi| < 1e-4."""
     meta, z = load_golden(name)
     out = {}
