@@ -1,0 +1,89 @@
+"""The benchmark configurations at their full sizes.
+
+- C1: 512 x 512 honeycomb from noise, 2000 FP64 steps, against the CPU oracle.
+- C2: 2048 x 2048 honeycomb polycrystal with box optimisation, 5000 steps, FP32
+  against FP64.
+- C3: the 4096 x 4096 heterostructure, FP32 against FP64 over the first 100
+  steps of its (chaotic) transient, and exact conservation of both means.
+
+Measured on B200 when these bounds were set:
+
+| config | quantity | measured | bound |
+|---|---|---|---|
+| C1 | FP64 vs oracle, max abs dpsi | 7e-13 | 1e-10 |
+| C1 | FP64 vs oracle, relative d<f> | 2e-15 | 1e-12 |
+| C1 | FP32 vs FP64, relative d<f> | 4e-9 | 1e-7 |
+| C2 | FP32 vs FP64, relative d<f> per print | <= 3e-9 | 1e-7 |
+| C2 | FP32 vs FP64, box size | 2e-8 | 1e-6 |
+| C3 | FP32 vs FP64, relative d<f> at 100 steps | 1.3e-8 | 1e-6 |
+"""
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from pfc_b200 import lib, synth
+from pfc_b200 import params as P
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_c1_honeycomb_512_full_run():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+    N, dx = 512, math.pi / 4
+    f0 = synth.noise_state(N, N, 0.25, 0.05, 0)[None]
+    with lib.Relaxation(p, N, N, dx, dx, "fp64") as g64, lib.Relaxation(p, N, N, dx, dx, "fp32") as g32:
+        o = pyoracle.Oracle(p, N, N, dx, dx)
+        for r in (g64, g32, o):
+            r.upload(f0)
+            r.step(2000)
+        a, b, c = g64.download(), g32.download(), o.download()
+        fa, fb, fc = g64.evaluate()[0], g32.evaluate()[0], o.evaluate()[0]
+        o.close()
+    assert np.abs(a - c).max() < 1e-10
+    assert abs(fa - fc) < 1e-12 * abs(fc)
+    assert abs(fb - fa) < 1e-7 * abs(fa)
+    assert fc < 0.0220  # relaxed well below the initial 0.0244 (10 steps)
+
+
+def test_c2_polycrystal_2048_box_optimisation():
+    p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+    N, dx = 2048, math.pi / 4
+    # 32 seeded grains, psi = 0.25 + A sum_j cos(q_j r) with A = -0.2 (the OMA here is half that sum)
+    f0 = synth.polycrystal(N, N, dx, dx, 32, 0.25, -0.4, 0.01, 0)[None]
+    rows = {}
+    for prec in ("fp64", "fp32"):
+        with lib.Relaxation(p, N, N, dx, dx, prec) as r:
+            r.upload(f0)
+            rows[prec] = r.relax(5000, 500, 100)
+    a, b = rows["fp64"], rows["fp32"]
+    assert a.shape == b.shape and a[-1, 0] == 5000
+    for x, y in zip(a[1:], b[1:]):
+        assert abs(x[3] - y[3]) < 1e-7 * abs(x[3])       # <f>
+        assert abs(x[1] - y[1]) < 1e-6 * x[1]             # dx after optimisation
+        assert abs(x[2] - y[2]) < 1e-6 * x[2]             # dy
+        assert abs(x[4] - y[4]) < 1e-14                   # the mean is conserved exactly
+    assert a[-1, 3] < a[0, 3] and a[-1, 1] != a[0, 1]     # relaxed, and the box did move
+
+
+def test_c3_heterostructure_4096_transient_and_means():
+    pd = P.hetero_2c(0.04)
+    p = P.make_params(pd, 1.0, 0.25)
+    N, dx, a0 = 4096, 0.7, 7.2552
+    f0 = synth.stripes2(N, N, dx, dx, 512, (0.3, -0.3), (0.3, 0.3), (a0, a0 * 1.04), 0.02, 1000)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        with lib.Relaxation(p, N, N, dx, dx, prec) as r:
+            r.upload(f0)
+            f_start, n_start = r.evaluate()
+            r.step(100)
+            out[prec] = r.evaluate()
+            assert np.array_equal(out[prec][1], n_start)    # both means bit for bit
+    assert abs(out["fp32"][0] - out["fp64"][0]) < 1e-6 * abs(out["fp64"][0])
