@@ -68,10 +68,19 @@ typedef struct pfcg_params {
 
 typedef struct pfcg_handle pfcg_handle;
 
-/* 1 if an Nx x Ny grid is supported (both even, 8 <= N <= 8192, N = 2^a 3^b 5^c 7^d),
- * else 0. The reference accepts any size through FFTW; sizes outside this set
- * are rejected with PFCG_ESIZE instead of falling back to a CPU path. */
+/* 1 if an Nx x Ny grid has a supported shape (both even, 8 <= N <= 8192,
+ * N = 2^a 3^b 5^c 7^d), else 0: a necessary condition. The reference accepts
+ * any size through FFTW; sizes outside this set are rejected with PFCG_ESIZE
+ * instead of falling back to a CPU path. */
 int pfcg_size_supported(int Nx, int Ny);
+
+/* 1 if pfcg_create accepts an Nx x Ny grid of U fields in precision prec, else
+ * 0 (no device work). Beyond the shape rules above, a transform of length N
+ * runs in one CTA: a radix-r pass needs N/r <= 512 * floor(16/r) butterflies
+ * (so 8192 with factors 2 only, 7168 with a 7, 7680 with a 3 or 5), and the U
+ * fields of one column (y-pass) or the channel pairs of one row (x-pass) must
+ * fit in shared memory (e.g. FP64 with U = 2 up to Ny of about 5600). */
+int pfcg_size_supported_for(int Nx, int Ny, int U, pfcg_prec prec);
 
 /* Creates a relaxation of U = p->U fields on an Nx x Ny grid with spacing dx, dy.
  * Replaces initialize() minus read_data: allocate_data (:162-193), plan_FFTs

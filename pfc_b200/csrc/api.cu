@@ -729,6 +729,22 @@ int pfcg_size_supported(int Nx, int Ny) {
 	return factor_ok(Nx) && factor_ok(Ny);
 }
 
+int pfcg_size_supported_for(int Nx, int Ny, int U, pfcg_prec prec) {
+	if (!pfcg_size_supported(Nx, Ny) || U < 1 || U > PFCG_MAX_U || (prec != PFCG_FP32 && prec != PFCG_FP64)) return 0;
+	// the layout checks pfcg_create makes, on a handle that is never allocated;
+	// the smallest tile and column group fit whenever any does
+	pfcg_handle h;
+	h.prec = prec;
+	h.U = U;
+	h.Nx = Nx;
+	h.Ny = Ny;
+	h.H = Nx / 2 + 1;
+	h.celem = prec == PFCG_FP64 ? sizeof(double2) : sizeof(float2);
+	if (!make_plan(Nx, max_radix(prec == PFCG_FP64), &h.px) || !make_plan(Ny, max_radix(prec == PFCG_FP64), &h.py))
+		return 0;
+	return x_tile_ok(&h, 1) && y_group_ok(&h, 1);
+}
+
 int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg_prec prec, pfcg_handle** out) {
 	if (!out) return fail(nullptr, PFCG_EARG, "out is NULL");
 	*out = nullptr;
@@ -799,9 +815,11 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	rc = fp64 ? upload_twiddles<double>(h, Nx, &h->twx) : upload_twiddles<float>(h, Nx, &h->twx);
 	if (!rc) rc = fp64 ? upload_twiddles<double>(h, Ny, &h->twy) : upload_twiddles<float>(h, Ny, &h->twy);
 	if (!rc && h->cxs.spec)
-		rc = fp64 ? upload_ct_twiddles<double>(h, Nx, rmain, &h->twctx) : upload_ct_twiddles<float>(h, Nx, rmain, &h->twctx);
+		rc = fp64 ? upload_ct_twiddles<double>(h, Nx, ct_radix(true), &h->twctx)
+		          : upload_ct_twiddles<float>(h, Nx, ct_radix(false), &h->twctx);
 	if (!rc && h->cys.spec)
-		rc = fp64 ? upload_ct_twiddles<double>(h, Ny, rmain, &h->twcty) : upload_ct_twiddles<float>(h, Ny, rmain, &h->twcty);
+		rc = fp64 ? upload_ct_twiddles<double>(h, Ny, ct_radix(true), &h->twcty)
+		          : upload_ct_twiddles<float>(h, Ny, ct_radix(false), &h->twcty);
 	if (rc) return bail(rc);
 	*out = h;
 	return 0;

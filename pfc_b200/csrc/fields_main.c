@@ -88,8 +88,8 @@ int main(int argc, char** argv) {
 		fprintf(stderr, "%s\n", pfcg_last_error(NULL));
 		return 1;
 	}
-	if (!pfcg_size_supported((int)W, (int)H)) {
-		fprintf(stderr, "grid size not supported by pfc_b200 (need even sizes 8..8192 with prime factors 2, 3, 5, 7).\n");
+	if (!pfcg_size_supported_for((int)W, (int)H, 2, PFCG_FP64)) {
+		fprintf(stderr, "grid size not supported by pfc_b200 (see pfcg_size_supported_for).\n");
 		return 42;
 	}
 	double* psi = (double*)malloc(sizeof(double) * 2 * n);

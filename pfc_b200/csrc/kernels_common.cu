@@ -3,8 +3,9 @@
 
 namespace pfcg {
 
-int max_elems_per_thread(bool fp64) { return fp64 ? FftCfg<double>::MAXE : FftCfg<float>::MAXE; }
-int max_radix(bool fp64) { return fp64 ? 8 : 16; }
+int max_elems_per_thread(bool fp64) { (void)fp64; return RT_MAXE; }
+int max_radix(bool fp64) { (void)fp64; return RT_MAXE; }
+int ct_radix(bool fp64) { return fp64 ? FftCfg<double>::MAXE : FftCfg<float>::MAXE; }
 
 int spec_rows(bool fp64, int U, int N) {
 	if ((U != 1 && U != 2) || (N != 2048 && N != 4096)) return 0;
@@ -19,14 +20,14 @@ template <typename T> static int ct_twn(int N) { return N == 4096 ? CtPlan<4096,
 int spec_twiddles(bool fp64, int N) { return fp64 ? ct_twn<double>(N) : ct_twn<float>(N); }
 
 int spec_x_threads(bool fp64, int U, int N) {
-	const int maxe = max_elems_per_thread(fp64);
+	const int maxe = ct_radix(fp64);
 	const int P = (U * spec_rows(fp64, U, N) + 1) / 2;
 	return P * N / maxe <= MAXNT ? P * N / maxe : MAXNT;
 }
 int spec_y_threads(bool fp64, int U, int N, bool fused) {
 	// fused y-pass: one thread per (field, column, butterfly); otherwise as many
 	// sequences per FFT call as fit MAXNT threads
-	const int maxe = max_elems_per_thread(fp64);
+	const int maxe = ct_radix(fp64);
 	const int S = U * spec_cols(fp64, U, N);
 	if (fused && U <= 2 && S * N / maxe <= MAXNT) return S * N / maxe;
 	if (S * N / maxe <= MAXNT) return S * N / maxe;

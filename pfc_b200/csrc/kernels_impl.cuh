@@ -24,9 +24,13 @@ namespace pfcg {
 
 // Elements a thread holds during one FFT pass (and the largest radix):
 // 16 in FP32, 8 in FP64, so the butterfly inputs take 32 registers either way.
+// Elements per thread (= main radix) of the compile-time specialised kernels
 template <typename T> struct FftCfg;
 template <> struct FftCfg<float> { static constexpr int MAXE = 16; };
 template <> struct FftCfg<double> { static constexpr int MAXE = 8; };
+// and of the runtime-plan kernels, in both precisions: 16 elements per thread
+// let 512 threads hold one 8192-point sequence (and 7168 / 7680 with a factor 7 / 5)
+constexpr int RT_MAXE = 16;
 constexpr int MAXNT = 512; // threads per CTA of the FFT kernels
 
 
@@ -107,7 +111,7 @@ __device__ __forceinline__ float phi1f(float x, float A) {
 // runtime length and plan). P / S resident sequences, NSUB per FFT call, NT threads.
 template <typename T, int U, int NC, int RC> struct XCfg {
 	static constexpr bool CT = NC > 0;
-	static constexpr int MAXE = FftCfg<T>::MAXE;
+	static constexpr int MAXE = CT ? FftCfg<T>::MAXE : RT_MAXE;
 	static constexpr int P = CT ? (U * RC + 1) / 2 : 1;
 	static constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
 	static constexpr int NSUB = CT ? (P * NC / MAXE <= MAXNT ? P : MAXNT * MAXE / NC) : 1;
@@ -118,7 +122,7 @@ template <typename T, int U, int NC, int RC> struct XCfg {
 
 template <typename T, int U, int NC, int CCC, int RC, bool FUSEDK = true> struct YCfg {
 	static constexpr bool CT = NC > 0;
-	static constexpr int MAXE = FftCfg<T>::MAXE;
+	static constexpr int MAXE = CT ? FftCfg<T>::MAXE : RT_MAXE;
 	static constexpr int S = CT ? U * CCC : 1;
 	static constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
 	static constexpr bool FUSED = FUSEDK && CT && CtPlan<(CT ? NC : 256), MAXE>::FUSABLE && U <= 2 &&

@@ -458,11 +458,14 @@ int main(int argc, char** argv) {
 			}
 		return 0;
 	}
-	if (!pfcg_size_supported(s.Nx, s.Ny))
-		die_msg(E_UNSUPPORTED, "grid size not supported by pfc_b200 (need even sizes 8..8192 with prime factors 2, 3, 5, 7).");
-
 	const char* pe = getenv("PFC_B200_PRECISION");
 	const pfcg_prec prec = (pe && strcmp(pe, "fp32") == 0) ? PFCG_FP32 : PFCG_FP64;
+	if (!pfcg_size_supported(s.Nx, s.Ny))
+		die_msg(E_UNSUPPORTED, "grid size not supported by pfc_b200 (need even sizes 8..8192 with prime factors 2, 3, 5, 7).");
+	if (!pfcg_size_supported_for(s.Nx, s.Ny, s.U, prec))
+		die_msg(E_UNSUPPORTED, prec == PFCG_FP64 ? "grid size not supported by pfc_b200 in FP64 for this many fields "
+		                                           "(see pfcg_size_supported_for; PFC_B200_PRECISION=fp32 supports more)."
+		                                         : "grid size not supported by pfc_b200 for this many fields.");
 	const char* de = getenv("PFC_B200_DEVICE");
 	check(pfcg_set_device(de ? atoi(de) : 0), NULL);
 

@@ -64,8 +64,9 @@ int main(int argc, char** argv) {
 		fprintf(stderr, "%s\n", pfcg_last_error(NULL));
 		return 1;
 	}
-	if (!pfcg_size_supported((int)W, (int)H)) {
-		fprintf(stderr, "grid size not supported by pfc_b200 (need even sizes 8..8192 with prime factors 2, 3, 5, 7).\n");
+	const char* pe0 = getenv("PFC_B200_PRECISION");
+	if (!pfcg_size_supported_for((int)W, (int)H, 1, (pe0 && strcmp(pe0, "fp32") == 0) ? PFCG_FP32 : PFCG_FP64)) {
+		fprintf(stderr, "grid size not supported by pfc_b200 (see pfcg_size_supported_for).\n");
 		return 42;
 	}
 	/* one field; only sigma matters for the smoothing */

@@ -30,6 +30,7 @@ NOALLOC_SCRATCH_BYTES = 32 << 20
 _vp, _ip, _dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "pfcg_size_supported": (ctypes.c_int, [_ip, _ip]),
+    "pfcg_size_supported_for": (ctypes.c_int, [_ip, _ip, _ip, _ip]),
     "pfcg_create": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, ctypes.c_double, ctypes.c_double, _ip,
                                    ctypes.POINTER(ctypes.c_void_p)]),
     "pfcg_upload": (ctypes.c_int, [_vp, _dp]),
@@ -111,6 +112,10 @@ def _dptr(a: np.ndarray):
 
 def size_supported(Nx: int, Ny: int) -> bool:
     return bool(load().pfcg_size_supported(Nx, Ny))
+
+
+def size_supported_for(Nx: int, Ny: int, U: int, precision: str) -> bool:
+    return bool(load().pfcg_size_supported_for(Nx, Ny, U, {"fp32": FP32, "fp64": FP64}[precision]))
 
 
 def set_device(device: int) -> None:

@@ -37,3 +37,15 @@ def test_create_rejects_bad_arguments_without_gpu_work():
     with pytest.raises(lib.PfcError) as e:
         lib.Relaxation(p, 66, 64, 0.7, 0.7)
     assert e.value.code == lib.ESIZE
+
+
+@pytest.mark.parametrize("Nx,Ny,U,prec,ok", [
+    (8192, 8, 1, lib.FP64, 1), (8192, 8, 1, lib.FP32, 1), (7168, 8, 2, lib.FP64, 1),
+    (8064, 8, 1, lib.FP32, 0),          # 8064 / 7 = 1152 butterflies: more than 512 threads x 2
+    (8, 8192, 2, lib.FP64, 0),          # two FP64 columns of 8192 exceed shared memory
+    (8, 8192, 2, lib.FP32, 1), (8192, 16, 4, lib.FP64, 0), (8192, 16, 4, lib.FP32, 1),
+    (4096, 4096, 4, lib.FP64, 0),       # four FP64 columns of 4096 exceed shared memory
+    (2048, 2048, 4, lib.FP64, 1), (30, 42, 3, lib.FP64, 1), (66, 64, 1, lib.FP32, 0), (64, 64, 0, lib.FP32, 0)])
+def test_size_supported_for(Nx, Ny, U, prec, ok):
+    """The exact host-side check of what pfcg_create accepts (no device work)."""
+    assert lib.load().pfcg_size_supported_for(Nx, Ny, U, prec) == ok

@@ -206,10 +206,13 @@ def test_specialised_sizes_match_oracle(U, N, steps):
         assert rel(fg, fo) < etol, (prec, rel(fg, fo))
 
 
-@pytest.mark.parametrize("U,Nx,Ny", [(1, 8192, 8), (2, 8, 8192), (1, 7000, 12), (2, 10, 6174), (1, 8192, 40)])
+@pytest.mark.parametrize("U,Nx,Ny", [(1, 8192, 8), (2, 8, 8192), (1, 7000, 12), (2, 10, 6174), (1, 8192, 40),
+                                      (2, 7168, 8)])
 def test_extreme_shapes_match_oracle(U, Nx, Ny):
-    """The longest supported transforms (8192), the shortest (8), ragged aspect
-    ratios and the 5/7 radices, FP64 and FP32, against the CPU oracle."""
+    """The longest supported transforms (8192; 7168 with a factor 7), the
+    shortest (8), ragged aspect ratios and the 5/7 radices against the CPU
+    oracle, in each precision pfcg_size_supported_for accepts; where it refuses,
+    pfcg_create refuses too."""
     dx, dy = 0.7, 0.65
     if U == 1:
         p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
@@ -218,6 +221,7 @@ def test_extreme_shapes_match_oracle(U, Nx, Ny):
         p = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
         f0 = np.array([synth.noise_state(Nx, Ny, m, 0.05, 32, stream=u) for u, m in enumerate((0.3, -0.3))])
     assert lib.size_supported(Nx, Ny)
+    assert lib.size_supported_for(Nx, Ny, U, "fp32")  # every shape here fits in FP32
     o = pyoracle.Oracle(p, Nx, Ny, dx, dy)
     o.upload(f0)
     o.step(5)
@@ -225,6 +229,11 @@ def test_extreme_shapes_match_oracle(U, Nx, Ny):
     fo, _ = o.evaluate()
     o.close()
     for prec, tol, etol in (("fp64", 1e-12, 1e-12), ("fp32", 2e-5, 1e-6)):
+        if not lib.size_supported_for(Nx, Ny, U, prec):
+            with pytest.raises(lib.PfcError) as e:
+                lib.Relaxation(p, Nx, Ny, dx, dy, prec)
+            assert e.value.code == lib.ESIZE
+            continue
         with lib.Relaxation(p, Nx, Ny, dx, dy, prec) as r:
             r.upload(f0)
             r.step(5)
