@@ -136,26 +136,46 @@ __global__ void dft_x(const float* __restrict__ in, float2* __restrict__ out, co
 	}
 }
 
-// out[r][x] (+)= sum_m scale[m] Re(in[r][m] exp(+2 pi i m x / T))
+// out[r][x] (+)= sum_m scale[m] Re(in[r][m] exp(+2 pi i m x / T)); each thread
+// makes four consecutive points of a row from one load of its MX modes
 __global__ void idft_x(const float2* __restrict__ in, float* __restrict__ out, const float2* __restrict__ tw,
                        const float* __restrict__ scale, long long nrows, int T, int accumulate) {
 	__shared__ float2 sh[MAXT];
 	__shared__ float sc[MX];
 	if (threadIdx.x < MX) sc[threadIdx.x] = scale ? scale[threadIdx.x] : 1.f;
 	load_tw(sh, tw, T);
-	const long long n = nrows * T;
+	const int q4 = T / 4;
+	const long long n = nrows * q4;
 	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-		const long long r = t / T;
-		const int x = (int)(t - r * T);
-		const float2* row = in + r * MX;
-		float acc = 0.f;
+		const long long r = t / q4;
+		const int x0 = (int)(t - r * q4) * 4;
+		float2 zm[MX];
 #pragma unroll
 		for (int m = 0; m < MX; m++) {
-			const float2 e = sh[(m * x) & (T - 1)];
-			const float2 z = row[m];
-			acc += sc[m] * (z.x * e.x - z.y * e.y);
+			const float2 z = in[r * MX + m];
+			zm[m] = make_float2(sc[m] * z.x, sc[m] * z.y);
 		}
-		out[t] = accumulate ? out[t] + acc : acc;
+		float acc[4];
+#pragma unroll
+		for (int k = 0; k < 4; k++) {
+			float a = 0.f;
+#pragma unroll
+			for (int m = 0; m < MX; m++) {
+				const float2 e = sh[(m * (x0 + k)) & (T - 1)];
+				a += zm[m].x * e.x - zm[m].y * e.y;
+			}
+			acc[k] = a;
+		}
+		float4* o4 = reinterpret_cast<float4*>(out + r * T + x0);
+		float4 res = make_float4(acc[0], acc[1], acc[2], acc[3]);
+		if (accumulate) {
+			const float4 p = *o4;
+			res.x += p.x;
+			res.y += p.y;
+			res.z += p.z;
+			res.w += p.w;
+		}
+		*o4 = res;
 	}
 }
 
@@ -234,13 +254,15 @@ __global__ void mix_grad(const float2* __restrict__ X, const float2* __restrict_
 	}
 }
 
-// z = W v + b + s; out = gelu(z) (act) or z. One thread per pixel.
+// z = W v + b + s; out = gelu(z) (act) or z. One thread per pixel; W rows are
+// read from shared memory four weights at a time.
 __global__ void __launch_bounds__(128) pointwise_fwd(const float* __restrict__ v, const float* __restrict__ s,
                                                      const __nv_bfloat16* __restrict__ w, int l, float* __restrict__ z,
                                                      float* __restrict__ out, int B, int npix, int act) {
-	__shared__ float Ws[C][C];
+	__shared__ float4 Ws[C][C / 4];
 	__shared__ float bs[C];
-	for (int i = threadIdx.x; i < C * C; i += blockDim.x) Ws[i / C][i % C] = wld(w, off_W(l) + i);
+	float* wsf = reinterpret_cast<float*>(Ws);
+	for (int i = threadIdx.x; i < C * C; i += blockDim.x) wsf[i] = wld(w, off_W(l) + i);
 	for (int i = threadIdx.x; i < C; i += blockDim.x) bs[i] = wld(w, off_b(l) + i);
 	__syncthreads();
 	const long long n = (long long)B * npix;
@@ -254,19 +276,27 @@ __global__ void __launch_bounds__(128) pointwise_fwd(const float* __restrict__ v
 		for (int o = 0; o < C; o++) {
 			float acc = bs[o] + s[base + (long long)o * npix];
 #pragma unroll
-			for (int i = 0; i < C; i++) acc += Ws[o][i] * in[i];
+			for (int q = 0; q < C / 4; q++) {
+				const float4 wq = Ws[o][q];
+				acc += wq.x * in[4 * q] + wq.y * in[4 * q + 1] + wq.z * in[4 * q + 2] + wq.w * in[4 * q + 3];
+			}
 			if (z) z[base + (long long)o * npix] = acc;
 			out[base + (long long)o * npix] = act ? gelu(acc) : acc;
 		}
 	}
 }
 
-// dz = dout * g'(z) (also the gradient of the spectral branch); dv = W^T dz
+// dz = dout * g'(z) (also the gradient of the spectral branch); dv = W^T dz,
+// with W held transposed in shared memory and read four weights at a time
 __global__ void __launch_bounds__(128) pointwise_bwd(const float* __restrict__ z, const float* __restrict__ dout,
                                                      const __nv_bfloat16* __restrict__ w, int l, float* __restrict__ dz,
                                                      float* __restrict__ dv, int B, int npix, int act) {
-	__shared__ float Ws[C][C];
-	for (int i = threadIdx.x; i < C * C; i += blockDim.x) Ws[i / C][i % C] = wld(w, off_W(l) + i);
+	__shared__ float4 WT[C][C / 4]; // WT[i][o / 4] = W[o .. o+3][i]
+	float* wtf = reinterpret_cast<float*>(WT);
+	for (int k = threadIdx.x; k < C * C; k += blockDim.x) {
+		const int o = k / C, i = k % C;
+		wtf[i * C + o] = wld(w, off_W(l) + k);
+	}
 	__syncthreads();
 	const long long n = (long long)B * npix;
 	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
@@ -283,7 +313,10 @@ __global__ void __launch_bounds__(128) pointwise_bwd(const float* __restrict__ z
 		for (int i = 0; i < C; i++) {
 			float acc = 0.f;
 #pragma unroll
-			for (int o = 0; o < C; o++) acc += Ws[o][i] * d[o];
+			for (int q = 0; q < C / 4; q++) {
+				const float4 wq = WT[i][q];
+				acc += wq.x * d[4 * q] + wq.y * d[4 * q + 1] + wq.z * d[4 * q + 2] + wq.w * d[4 * q + 3];
+			}
 			dv[base + (long long)i * npix] = acc;
 		}
 	}
@@ -610,7 +643,7 @@ int forward(pfcg_fno* f, const float* x, int B, const float* target, bool train)
 		dft_y<<<planes_grid(planes), 128, 0, st>>>(f->A, f->X[l], f->tw, planes, T, 0);
 		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->w, l, B, 0);
 		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Y, f->Bq, f->tw, planes, T, 1);
-		idft_x<<<grid_for(rows * T, 256), 256, 0, st>>>(f->Bq, f->s, f->tw, f->sx, rows, T, 0);
+		idft_x<<<grid_for(rows * T / 4, 256), 256, 0, st>>>(f->Bq, f->s, f->tw, f->sx, rows, T, 0);
 		pointwise_fwd<<<grid_for((long long)B * npix, 128), 128, 0, st>>>(f->v[l], f->s, f->w, l, train ? f->z[l] : nullptr,
 		                                                                    f->v[l + 1], B, npix, l < L - 1);
 		f->launches += 6;
@@ -645,7 +678,7 @@ int backward(pfcg_fno* f, const float* x, int B) {
 		mix_grad<<<grid_for((long long)C * C * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->g, l, B);
 		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->Y, f->Bq, f->w, l, B, 1);
 		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Bq, f->A, f->tw, planes, T, 1);
-		idft_x<<<grid_for(rows * T, 256), 256, 0, st>>>(f->A, f->dv2, f->tw, nullptr, rows, T, 1);
+		idft_x<<<grid_for(rows * T / 4, 256), 256, 0, st>>>(f->A, f->dv2, f->tw, nullptr, rows, T, 1);
 		f->launches += 8;
 		std::swap(f->dv, f->dv2);
 	}
