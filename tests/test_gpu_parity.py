@@ -239,3 +239,56 @@ def test_extreme_shapes_match_oracle(U, Nx, Ny):
             r.step(5)
             assert np.abs(r.download() - ref).max() < tol, prec
             assert rel(r.evaluate()[0], fo) < etol, prec
+
+
+def four_fields():
+    """Four coupled fields (the most pfcg_params holds): the three-field
+    heterostructure plus a fourth field with two modes, coupled to the first by
+    smoothed-density (epsilon) and gradient (beta, mu) terms and to the third by
+    alpha and gamma."""
+    from golden.make_golden import hetero_3c
+
+    d = hetero_3c()
+    U = 4
+    grow = lambda m, fill=0.0: [row + [fill] for row in m] + [[0.0] * U]  # noqa: E731
+    d["alpha"] = grow(d["alpha"])
+    d["alpha"][3][3] = -0.2
+    d["alpha"][2][3] = 0.1
+    d["beta"] = grow(d["beta"])
+    d["beta"][3][3] = 1.0
+    d["beta"][0][3] = 0.02
+    d["gamma"] = grow(d["gamma"])
+    d["gamma"][2][3] = 0.2
+    d["epsilon"] = grow(d["epsilon"])
+    d["epsilon"][0][3] = -0.5
+    d["inv_mu"] = grow(d["inv_mu"])
+    d["inv_mu"][0][3] = 1.05
+    d["lambda"] = d["lambda"] + [0.0]
+    d["delta"] = d["delta"] + [1.0]
+    d["inv_nu"] = d["inv_nu"] + [[1.0, 2.0 ** 0.5]]
+    d["omega"] = d["omega"] + [[1.0, 1.0]]
+    d["phi"] = d["phi"] + [[0.0, 0.05]]
+    return d
+
+
+@pytest.mark.parametrize("Nx,Ny", [(64, 48), (80, 60)])
+def test_four_fields_match_oracle(Nx, Ny):
+    dx = dy = 0.7
+    p = P.make_params(four_fields(), 1.0, 0.25)
+    f0 = np.array([synth.noise_state(Nx, Ny, m, 0.1, 41, stream=u) for u, m in enumerate((0.485, -0.32, -0.32, 0.1))])
+    o = pyoracle.Oracle(p, Nx, Ny, dx, dy)
+    o.upload(f0)
+    with lib.Relaxation(p, Nx, Ny, dx, dy, "fp64") as r64, lib.Relaxation(p, Nx, Ny, dx, dy, "fp32") as r32:
+        r64.upload(f0)
+        r32.upload(f0)
+        for chunk in (1, 9, 20):
+            assert o.step(chunk) == 0
+            r64.step(chunk)
+            r32.step(chunk)
+            ref = o.download()
+            np.testing.assert_allclose(r64.download(), ref, rtol=0, atol=1e-11)
+            assert np.abs(r32.download() - ref).max() < 2e-5
+            fo, no = o.evaluate()
+            assert rel(r64.evaluate()[0], fo) < 1e-11
+            assert rel(r32.evaluate()[0], fo) < 1e-6
+            np.testing.assert_allclose(r64.evaluate()[1], no, rtol=1e-12, atol=1e-14)
