@@ -253,14 +253,14 @@ int choose_layout(pfcg_handle* h, int nsm) {
 // CtPlan): passes of radix rmain with the tail radix second; pass p > 0 contributes
 // entries [(r - 1) * Ns + jm] = exp(-2 pi i r jm / (Ns R)).
 template <typename T> int upload_ct_twiddles(pfcg_handle* h, int N, int rmain, void** dst) {
-	int lg = 0;
-	while ((1 << lg) < N) lg++;
-	int lgm = 0;
-	while ((1 << lgm) < rmain) lgm++;
-	// the tail radix is the second pass (fft_core.cuh, CtPlan)
+	// N = rmain^A * tail; the tail radix is the second pass (fft_core.cuh, CtPlan)
 	std::vector<int> radix;
-	for (int i = 0; i < lg / lgm; i++) radix.push_back(rmain);
-	if (lg % lgm) radix.insert(radix.begin() + (radix.empty() ? 0 : 1), 1 << (lg % lgm));
+	int rest = N;
+	while (rest % rmain == 0) {
+		radix.push_back(rmain);
+		rest /= rmain;
+	}
+	if (rest > 1) radix.insert(radix.begin() + (radix.empty() ? 0 : 1), rest);
 	std::vector<cplx<T>> tab;
 	int Ns = 1;
 	for (size_t p = 0; p < radix.size(); p++) {

@@ -144,6 +144,28 @@ template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft3(cp
 	v[2] = csub(m1, m2);
 }
 
+// Length 6 = 2 x 3 by the prime-factor (Good-Thomas) index map, which needs no
+// twiddles: input n = (3 n1 + 2 n2) mod 6, output k = (3 k1 + 4 k2) mod 6, and
+// exp(SIGN 2 pi i n k / 6) = (-1)^(n1 k1) exp(SIGN 2 pi i n2 k2 / 3).
+template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft6(cplx<T>* v) {
+	cplx<T> b0[3] = {v[0], v[2], v[4]}; // k1 = 0: sums over n1
+	cplx<T> b1[3] = {v[0], v[2], v[4]}; // k1 = 1: differences
+	const cplx<T> o[3] = {v[3], v[5], v[1]};
+#pragma unroll
+	for (int n2 = 0; n2 < 3; n2++) {
+		b0[n2] = cadd(b0[n2], o[n2]);
+		b1[n2] = csub(b1[n2], o[n2]);
+	}
+	dft3<SIGN, T>(b0);
+	dft3<SIGN, T>(b1);
+	v[0] = b0[0];
+	v[4] = b0[1];
+	v[2] = b0[2];
+	v[3] = b1[0];
+	v[1] = b1[1];
+	v[5] = b1[2];
+}
+
 template <int SIGN, typename T> __host__ __device__ __forceinline__ void dft5(cplx<T>* v) {
 	const T c1 = (T)0.30901699437494742410229341718282;  // cos(2pi/5)
 	const T c2 = (T)-0.80901699437494742410229341718282; // cos(4pi/5)
@@ -199,6 +221,7 @@ template <int R, int SIGN, typename T> __host__ __device__ __forceinline__ void 
 	else if constexpr (R == 3) dft3<SIGN, T>(v);
 	else if constexpr (R == 4) dft4<SIGN, T>(v);
 	else if constexpr (R == 5) dft5<SIGN, T>(v);
+	else if constexpr (R == 6) dft6<SIGN, T>(v);
 	else if constexpr (R == 7) dft7<SIGN, T>(v);
 	else if constexpr (R == 8) dft8<SIGN, T>(v);
 	else if constexpr (R == 16) dft16<SIGN, T>(v);
@@ -312,14 +335,17 @@ __device__ __forceinline__ void fft_batches(cplx<T>* buf, int ld, int S, int SB,
 
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
 
-// The tail radix, when there is one, is pass 1 (second), so that the first and
-// the last pass both have radix RM: the last pass then leaves in each thread
-// exactly the elements the next transform's first pass needs (fused below).
+// N = RM^A * RT with RM^(A+1) not dividing N; RT (1 = none) is one of the
+// radices dft() has (2, 3, 4, 6, 8 for the lengths used). The tail radix, when
+// there is one, is pass 1 (second), so that the first and the last pass both
+// have radix RM: the last pass then leaves in each thread exactly the elements
+// the next transform's first pass needs (fused below).
+__host__ __device__ constexpr int ct_count(int n, int r) { return (n > 0 && n % r == 0) ? 1 + ct_count(n / r, r) : 0; }
+__host__ __device__ constexpr int ct_ipow(int b, int e) { return e == 0 ? 1 : b * ct_ipow(b, e - 1); }
 template <int N, int RM> struct CtPlan {
-	static constexpr int LG = ilog2(N);
-	static constexpr int LGM = ilog2(RM);
-	static constexpr int A = LG / LGM;                 // passes of radix RM
-	static constexpr int RT = 1 << (LG % LGM);         // tail radix (1 = none)
+	static constexpr int A = ct_count(N, RM);          // passes of radix RM
+	static constexpr int RT = N / ct_ipow(RM, A);      // tail radix (1 = none)
+	static_assert(N == 0 || RT == 1 || RT == 2 || RT == 3 || RT == 4 || RT == 6 || RT == 8, "no DFT for this tail radix");
 	static constexpr int NPASS = A + (RT > 1 ? 1 : 0);
 	static constexpr bool FUSABLE = A >= 2;            // first and last pass both radix RM
 	__host__ __device__ static constexpr int radix(int p) { return (RT > 1 && p == 1) ? RT : RM; }

@@ -7,16 +7,27 @@ int max_elems_per_thread(bool fp64) { (void)fp64; return RT_MAXE; }
 int max_radix(bool fp64) { (void)fp64; return RT_MAXE; }
 int ct_radix(bool fp64) { return fp64 ? FftCfg<double>::MAXE : FftCfg<float>::MAXE; }
 
-int spec_rows(bool fp64, int U, int N) {
-	if ((U != 1 && U != 2) || (N != 2048 && N != 4096)) return 0;
-	return fp64 ? Spec<double>::xr(U, N) : Spec<float>::xr(U, N);
-}
-int spec_cols(bool fp64, int U, int N) {
-	if ((U != 1 && U != 2) || (N != 2048 && N != 4096)) return 0;
-	return fp64 ? Spec<double>::ycc(U, N) : Spec<float>::ycc(U, N);
-}
+// 0 where the size has no specialised kernel (Spec in kernels_impl.cuh)
+int spec_rows(bool fp64, int U, int N) { return fp64 ? Spec<double>::xr(U, N) : Spec<float>::xr(U, N); }
+int spec_cols(bool fp64, int U, int N) { return fp64 ? Spec<double>::ycc(U, N) : Spec<float>::ycc(U, N); }
 
-template <typename T> static int ct_twn(int N) { return N == 4096 ? CtPlan<4096, FftCfg<T>::MAXE>::TWN : CtPlan<2048, FftCfg<T>::MAXE>::TWN; }
+template <typename T> static int ct_twn(int N) {
+	constexpr int M = FftCfg<T>::MAXE;
+	switch (N) {
+	case 4096: return CtPlan<4096, M>::TWN;
+	case 2048: return CtPlan<2048, M>::TWN;
+	}
+	if constexpr (M == 16) {
+		switch (N) {
+		case 1536: return CtPlan<1536, M>::TWN;
+		case 1024: return CtPlan<1024, M>::TWN;
+		case 768: return CtPlan<768, M>::TWN;
+		case 512: return CtPlan<512, M>::TWN;
+		case 256: return CtPlan<256, M>::TWN;
+		}
+	}
+	return 0;
+}
 int spec_twiddles(bool fp64, int N) { return fp64 ? ct_twn<double>(N) : ct_twn<float>(N); }
 
 int spec_x_threads(bool fp64, int U, int N) {

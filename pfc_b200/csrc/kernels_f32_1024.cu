@@ -1,0 +1,11 @@
+// FP32 STEP kernels specialised on the length 1024 (kernels_impl.cuh: Spec, CtPlan),
+// U = 1 and 2; one file per length so that the lengths compile in parallel.
+#define PFCG_CT_TU 1024
+#include "kernels_impl.cuh"
+
+namespace pfcg {
+
+PFCG_CT_DECL(, 1, 1024)
+PFCG_CT_DECL(, 2, 1024)
+
+} // namespace pfcg

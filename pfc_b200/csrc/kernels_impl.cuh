@@ -1166,31 +1166,127 @@ static cudaError_t xlaunch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s
 // Compile-time specialisations of the STEP kernels: (length, rows per tile,
 // columns per y-pass CTA) for the sizes the workloads use; other sizes and
 // modes run the runtime-plan kernels.
+template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
+static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	auto k = ypass_kernel<T, U, MODE, NC, CCC, RC, FUSEDK>;
+	static unsigned long long mask = 0;
+	static int resident = 0;
+	smem_attr(k, mask);
+	const int grid = NC > 0 && std::is_same<T, double>::value ? resident_grid(k, c, resident) : c.grid;
+	k<<<grid, c.block, c.smem, s>>>(a, c.grid);
+	return cudaGetLastError();
+}
+
 template <typename T> struct Spec;
+// Rows per x-pass tile (xr) and columns per y-pass group (ycc) of the kernels
+// specialised on a compile-time length N, 0 where there is none. The row tile
+// is also the layout of `work` for the runtime-plan modes (evaluate, c2r, r2c),
+// so U * xr stays within MAX_CH: an FP32 x-pass CTA runs U * xr * N / 32
+// threads (512 at N = 4096 and 2048, N / 4 below). A y-pass CTA runs
+// U * ycc * N / 16 threads: 512, or 384 at N = 768 and 1536 (16^2 * 3, 16^2 * 6).
 template <> struct Spec<float> {
-	// U = 1: x rows 4 (4096) / 8 (2048), y columns 2 / 4; U = 2: x rows 2 / 4, y columns 1 / 2
-	static constexpr int xr(int U, int N) { return U == 1 ? (N == 4096 ? 4 : 8) : (N == 4096 ? 2 : 4); }
-	static constexpr int ycc(int U, int N) { return U == 1 ? (N == 4096 ? 2 : 4) : (N == 4096 ? 1 : 2); }
+	static constexpr int x1(int N) {
+		return N == 4096 ? 4 : (N == 2048 || N == 1536 || N == 1024 || N == 768 || N == 512 || N == 256) ? 8 : 0;
+	}
+	static constexpr int y1(int N) {
+		return N == 4096 ? 2 : N == 2048 || N == 1536 ? 4 : N == 1024 || N == 768 ? 8 : N == 512 ? 16 : N == 256 ? 32 : 0;
+	}
+	static constexpr int xr(int U, int N) { return U == 1 ? x1(N) : U == 2 ? x1(N) / 2 : 0; }
+	static constexpr int ycc(int U, int N) { return U == 1 ? y1(N) : U == 2 ? y1(N) / 2 : 0; }
 };
 template <> struct Spec<double> {
-	static constexpr int xr(int U, int N) { return U == 1 ? (N == 4096 ? 2 : 4) : (N == 4096 ? 1 : 2); }
-	static constexpr int ycc(int U, int N) { return U == 1 ? (N == 4096 ? 1 : 2) : 1; }
+	static constexpr int xr(int U, int N) {
+		return N == 4096 ? (U == 1 ? 2 : U == 2 ? 1 : 0) : N == 2048 ? (U == 1 ? 4 : U == 2 ? 2 : 0) : 0;
+	}
+	static constexpr int ycc(int U, int N) {
+		return N == 4096 ? (U == 1 ? 1 : U == 2 ? 1 : 0) : N == 2048 ? (U == 1 ? 2 : U == 2 ? 1 : 0) : 0;
+	}
 };
 
-template <typename T, int U, int N> static bool x_is_spec(const XArgs<T>& a) {
-	return a.g.Nx == N && a.g.R == Spec<T>::xr(U, N);
+template <typename T, int U> static bool x_is_spec(const XArgs<T>& a) {
+	return Spec<T>::xr(U, a.g.Nx) > 0 && a.g.R == Spec<T>::xr(U, a.g.Nx);
 }
-template <typename T, int U, int N> static bool y_is_spec(const YArgs<T>& a) {
-	return a.g.Ny == N && a.g.CC == Spec<T>::ycc(U, N) && a.g.R == Spec<T>::xr(U, N);
+template <typename T, int U> static bool y_is_spec(const YArgs<T>& a) {
+	return Spec<T>::ycc(U, a.g.Ny) > 0 && a.g.CC == Spec<T>::ycc(U, a.g.Ny) && a.g.R == Spec<T>::xr(U, a.g.Ny);
+}
+
+// STEP passes of the specialised kernels of length N. The FP32 lengths below
+// 2048 are instantiated in kernels_f32_<N>.cu, one file each, so that they
+// compile in parallel.
+template <typename T, int U, int N> cudaError_t ct_xstep(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	return xlaunch<T, U, XP_STEP, N, Spec<T>::xr(U, N)>(a, c, s);
+}
+template <typename T, int U, int N> cudaError_t ct_ystep(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	// c.spec: 1 = specialised (fused where possible), 2 = specialised, never fused
+	if (c.spec == 2) return ylaunch<T, U, YP_STEP, N, Spec<T>::ycc(U, N), Spec<T>::xr(U, N), false>(a, c, s);
+	return ylaunch<T, U, YP_STEP, N, Spec<T>::ycc(U, N), Spec<T>::xr(U, N)>(a, c, s);
+}
+
+#ifndef PFCG_CT_TU
+#define PFCG_CT_TU 0
+#endif
+#define PFCG_CT_DECL(EXT, U, N)                                                                                        \
+	EXT template cudaError_t ct_xstep<float, U, N>(const XArgs<float>&, const LaunchCfg&, cudaStream_t);               \
+	EXT template cudaError_t ct_ystep<float, U, N>(const YArgs<float>&, const LaunchCfg&, cudaStream_t);
+#if PFCG_CT_TU != 256
+PFCG_CT_DECL(extern, 1, 256)
+PFCG_CT_DECL(extern, 2, 256)
+#endif
+#if PFCG_CT_TU != 512
+PFCG_CT_DECL(extern, 1, 512)
+PFCG_CT_DECL(extern, 2, 512)
+#endif
+#if PFCG_CT_TU != 768
+PFCG_CT_DECL(extern, 1, 768)
+PFCG_CT_DECL(extern, 2, 768)
+#endif
+#if PFCG_CT_TU != 1024
+PFCG_CT_DECL(extern, 1, 1024)
+PFCG_CT_DECL(extern, 2, 1024)
+#endif
+#if PFCG_CT_TU != 1536
+PFCG_CT_DECL(extern, 1, 1536)
+PFCG_CT_DECL(extern, 2, 1536)
+#endif
+
+template <typename T, int U> static cudaError_t ct_xdispatch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	switch (a.g.Nx) {
+	case 4096: return ct_xstep<T, U, 4096>(a, c, s);
+	case 2048: return ct_xstep<T, U, 2048>(a, c, s);
+	}
+	if constexpr (std::is_same<T, float>::value) {
+		switch (a.g.Nx) {
+		case 1536: return ct_xstep<T, U, 1536>(a, c, s);
+		case 1024: return ct_xstep<T, U, 1024>(a, c, s);
+		case 768: return ct_xstep<T, U, 768>(a, c, s);
+		case 512: return ct_xstep<T, U, 512>(a, c, s);
+		case 256: return ct_xstep<T, U, 256>(a, c, s);
+		}
+	}
+	return cudaErrorInvalidValue;
+}
+template <typename T, int U> static cudaError_t ct_ydispatch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
+	switch (a.g.Ny) {
+	case 4096: return ct_ystep<T, U, 4096>(a, c, s);
+	case 2048: return ct_ystep<T, U, 2048>(a, c, s);
+	}
+	if constexpr (std::is_same<T, float>::value) {
+		switch (a.g.Ny) {
+		case 1536: return ct_ystep<T, U, 1536>(a, c, s);
+		case 1024: return ct_ystep<T, U, 1024>(a, c, s);
+		case 768: return ct_ystep<T, U, 768>(a, c, s);
+		case 512: return ct_ystep<T, U, 512>(a, c, s);
+		case 256: return ct_ystep<T, U, 256>(a, c, s);
+		}
+	}
+	return cudaErrorInvalidValue;
 }
 
 template <typename T, int U> static cudaError_t xlaunch_mode(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
 	switch (mode) {
 	case XP_STEP:
-		if constexpr (U <= 2) {
-			if (c.spec && x_is_spec<T, U, 4096>(a)) return xlaunch<T, U, XP_STEP, 4096, Spec<T>::xr(U, 4096)>(a, c, s);
-			if (c.spec && x_is_spec<T, U, 2048>(a)) return xlaunch<T, U, XP_STEP, 2048, Spec<T>::xr(U, 2048)>(a, c, s);
-		}
+		if constexpr (U <= 2)
+			if (c.spec && x_is_spec<T, U>(a)) return ct_xdispatch<T, U>(a, c, s);
 		return xlaunch<T, U, XP_STEP, 0, 0>(a, c, s);
 	case XP_EVAL: return xlaunch<T, U, XP_EVAL, 0, 0>(a, c, s);
 	case XP_C2R: return xlaunch<T, U, XP_C2R, 0, 0>(a, c, s);
@@ -1209,27 +1305,9 @@ template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, cons
 	return cudaErrorInvalidValue;
 }
 
-template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
-static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
-	auto k = ypass_kernel<T, U, MODE, NC, CCC, RC, FUSEDK>;
-	static unsigned long long mask = 0;
-	static int resident = 0;
-	smem_attr(k, mask);
-	const int grid = NC > 0 && std::is_same<T, double>::value ? resident_grid(k, c, resident) : c.grid;
-	k<<<grid, c.block, c.smem, s>>>(a, c.grid);
-	return cudaGetLastError();
-}
 
 template <typename T, int U> static cudaError_t ystep(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
-	// c.spec: 1 = specialised (fused where possible), 2 = specialised, never fused
-	if (c.spec && y_is_spec<T, U, 4096>(a)) {
-		if (c.spec == 2) return ylaunch<T, U, YP_STEP, 4096, Spec<T>::ycc(U, 4096), Spec<T>::xr(U, 4096), false>(a, c, s);
-		return ylaunch<T, U, YP_STEP, 4096, Spec<T>::ycc(U, 4096), Spec<T>::xr(U, 4096)>(a, c, s);
-	}
-	if (c.spec && y_is_spec<T, U, 2048>(a)) {
-		if (c.spec == 2) return ylaunch<T, U, YP_STEP, 2048, Spec<T>::ycc(U, 2048), Spec<T>::xr(U, 2048), false>(a, c, s);
-		return ylaunch<T, U, YP_STEP, 2048, Spec<T>::ycc(U, 2048), Spec<T>::xr(U, 2048)>(a, c, s);
-	}
+	if (c.spec && y_is_spec<T, U>(a)) return ct_ydispatch<T, U>(a, c, s);
 	return ylaunch<T, U, YP_STEP, 0, 0, 0>(a, c, s);
 }
 

@@ -181,7 +181,7 @@ def test_launches_per_step():
 
 @pytest.mark.parametrize("U,N,steps", [(1, 2048, 3), (2, 2048, 3), (1, 4096, 2), (2, 4096, 2)])
 def test_specialised_sizes_match_oracle(U, N, steps):
-    """The compile-time specialised STEP kernels (lengths 2048 and 4096) against
+    """The compile-time specialised STEP kernels of lengths 2048 and 4096 against
     the CPU oracle, FP64 and FP32."""
     dx = dy = 0.7
     if U == 1:
@@ -204,6 +204,41 @@ def test_specialised_sizes_match_oracle(U, N, steps):
             fg, _ = r.evaluate()
         assert np.abs(got - ref).max() < tol, (prec, np.abs(got - ref).max())
         assert rel(fg, fo) < etol, (prec, rel(fg, fo))
+
+
+@pytest.mark.parametrize("U", [1, 2])
+@pytest.mark.parametrize("N", [256, 512, 768, 1024, 1536])
+def test_specialised_fp32_lengths_match_oracle(U, N, monkeypatch):
+    """The FP32 STEP kernels specialised on the lengths below 2048 (radix 16 with
+    a tail pass of radix 1, 2, 3, 4 or 6) against the CPU oracle, beside the
+    runtime-plan kernels (PFCG_GENERIC_KERNELS=1) on the same state. The two
+    FP32 results differ in rounding only, which shows that a different
+    transform ran."""
+    dx = dy = 0.7
+    steps = 5
+    if U == 1:
+        p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+        f0 = synth.noise_state(N, N, 0.25, 0.05, 31)[None]
+    else:
+        p = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
+        f0 = synth.stripes2(N, N, dx, dy, N // 8, (0.3, -0.3), (0.3, 0.3), (7.2552, 7.2552 * 1.04), 0.02, 32)
+    o = pyoracle.Oracle(p, N, N, dx, dy)
+    o.upload(f0)
+    o.step(steps)
+    ref = o.download()
+    fo, _ = o.evaluate()
+    o.close()
+    got = {}
+    for generic in ("0", "1"):
+        monkeypatch.setenv("PFCG_GENERIC_KERNELS", generic)
+        with lib.Relaxation(p, N, N, dx, dy, "fp32") as r:
+            r.upload(f0)
+            r.step(steps)
+            got[generic] = r.download()
+            fg, _ = r.evaluate()
+        assert np.abs(got[generic] - ref).max() < 2e-5, (generic, np.abs(got[generic] - ref).max())
+        assert rel(fg, fo) < 1e-6, (generic, rel(fg, fo))
+    assert not np.array_equal(got["0"], got["1"])
 
 
 @pytest.mark.parametrize("U,Nx,Ny", [(1, 8192, 8), (2, 8, 8192), (1, 7000, 12), (2, 10, 6174), (1, 8192, 40),
