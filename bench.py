@@ -212,7 +212,8 @@ def run_batch(args):
         t0 = time.perf_counter()
         b.step(K)
         dt = time.perf_counter() - t0
-        res["batched"] = {"updates_per_s": upd * K / dt, "ms_per_step": dt / K * 1e3, "kernel_launches_per_step": 2,
+        res["batched"] = {"updates_per_s": upd * K / dt, "ms_per_step": dt / K * 1e3,
+                          "kernel_launches_per_step": b.launches(1)[0],
                           "graph_launches": 1}
         rs = [lib.Relaxation(*p[:5], "fp32") for p in probs]
     for r, p in zip(rs, probs):

@@ -197,10 +197,14 @@ int pfcg_profile_read(pfcg_handle* h, double* ms, long long* launches, int nkind
 int pfcg_autotune(pfcg_handle* h, int nsteps);
 
 /* Many independent relaxations (sizes, fields and parameters may differ)
- * stepped together: one step of all problems is two kernel launches (a batched
- * x-pass and a batched y-pass over per-problem tables), and pfcg_batch_step
- * captures nsteps of them into one CUDA graph (cached per nsteps) and launches
- * it. Problem i is an ordinary handle (pfcg_batch_problem) for upload,
+ * stepped together. The problems fall into classes: one per (U, N) with
+ * N = Nx = Ny a length with specialised kernels (pfcg_autotune lists them), in
+ * their fixed launch shape, and one for all other problems, on the
+ * runtime-plan kernels. A step of a class is two kernel launches (a batched
+ * x-pass and a batched y-pass over per-problem tables); pfcg_batch_step
+ * captures nsteps steps into one CUDA graph (cached per nsteps), each class a
+ * chain of its own that runs beside the others, and launches it.
+ * pfcg_batch_launches reports 2 * classes * nsteps kernels per graph launch. Problem i is an ordinary handle (pfcg_batch_problem) for upload,
  * evaluate, optimize and download; do not step it on its own while the batch is
  * in use. params is an array of nprob structs; autotune != 0 runs
  * pfcg_autotune on every problem first. No counterpart in the reference, which

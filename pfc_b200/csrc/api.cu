@@ -1169,56 +1169,123 @@ extern "C" int pfcg_autotune(pfcg_handle* h, int nsteps) {
 }
 
 // ------------------------------------------------------------------ batch ---
+// Problems of a batch that run the same kernels: one length N = Nx = Ny and
+// field count U with specialised kernels, or (ct = false) every other problem,
+// on the runtime-plan kernels. A class's blocks are a contiguous range of the
+// batch's block tables, and its steps form one chain of the step graph on its
+// own stream, independent of the other classes' chains.
+struct BatchClass {
+	bool ct = false;
+	int U = 0, N = 0;
+	LaunchCfg cx{}, cy{};      // ct: the specialised launch shapes of its problems
+	int threads = 0, smem = 0; // runtime-plan class: the largest of its problems'
+	int xoff = 0, xn = 0, yoff = 0, yn = 0;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t done = nullptr;
+};
+
 struct pfcg_batch {
 	pfcg_prec prec = PFCG_FP32;
 	std::vector<pfcg_handle*> h;
 	cudaStream_t stream = nullptr;
+	cudaEvent_t fork = nullptr;
 	void* d_xargs = nullptr;
 	void* d_yargs = nullptr;
 	int* d_blk = nullptr; // x problem, x local, y problem, y local tables
 	int* d_flags = nullptr;
 	int* h_flags = nullptr;
-	int xblocks = 0, yblocks = 0, threads = 0, smem = 0;
+	int xblocks = 0, yblocks = 0;
+	std::vector<BatchClass> cls;
 	std::map<int, cudaGraphExec_t> graphs;
 	std::string err;
 };
+
+// whether a batch problem runs the specialised kernels (decided at creation)
+static bool batch_ct(const pfcg_handle* h) { return h->cxs.spec && h->cys.spec && h->Nx == h->Ny && h->U <= 2; }
 
 namespace {
 
 template <typename T> int batch_build(pfcg_batch* b) {
 	const int n = (int)b->h.size();
+	auto bfail = [&](cudaError_t e, const char* what) {
+		b->err = std::string(what) + ": " + cudaGetErrorString(e);
+		return PFCG_ECUDA;
+	};
 	std::vector<XArgs<T>> xa(n);
 	std::vector<YArgs<T>> ya(n);
-	// blocks of the largest problems first, so the tail of the launch is short
-	std::vector<int> order(n);
-	for (int i = 0; i < n; i++) order[i] = i;
-	std::sort(order.begin(), order.end(), [&](int a, int c) {
-		return (long long)b->h[a]->Nx * b->h[a]->Ny * b->h[a]->U > (long long)b->h[c]->Nx * b->h[c]->Ny * b->h[c]->U;
-	});
-	std::vector<int> xp, xl, yp, yl;
-	b->threads = 32;
-	b->smem = 0;
 	for (int i = 0; i < n; i++) {
 		pfcg_handle* h = b->h[i];
 		xa[i] = xargs<T>(h);
 		xa[i].acc = h->acc + ACC_NL;
 		xa[i].flag = b->d_flags + i;
 		ya[i] = yargs<T>(h);
-		b->threads = std::max(b->threads, std::max(h->cx.block, h->cy.block));
-		b->smem = std::max(b->smem, std::max(h->cx.smem, h->cy.smem));
 	}
-	for (int i : order) {
-		for (int t = 0; t < b->h[i]->cx.grid; t++) { xp.push_back(i); xl.push_back(t); }
-		for (int g = 0; g < b->h[i]->cy.grid; g++) { yp.push_back(i); yl.push_back(g); }
+	// classes: one per (U, N) with specialised kernels, one for the rest
+	std::map<std::pair<int, int>, int> key;
+	std::vector<std::vector<int>> members;
+	int generic = -1;
+	for (int i = 0; i < n; i++) {
+		pfcg_handle* h = b->h[i];
+		int c;
+		if (batch_ct(h)) {
+			auto it = key.find({h->U, h->Nx});
+			if (it == key.end()) {
+				c = (int)b->cls.size();
+				key[{h->U, h->Nx}] = c;
+				BatchClass k;
+				k.ct = true;
+				k.U = h->U;
+				k.N = h->Nx;
+				k.cx = h->cxs;
+				k.cy = h->cys;
+				b->cls.push_back(k);
+				members.emplace_back();
+			} else {
+				c = it->second;
+			}
+		} else {
+			if (generic < 0) {
+				generic = (int)b->cls.size();
+				b->cls.push_back(BatchClass{});
+				b->cls.back().threads = 32;
+				members.emplace_back();
+			}
+			c = generic;
+			BatchClass& k = b->cls[c];
+			k.threads = std::max(k.threads, std::max(h->cx.block, h->cy.block));
+			k.smem = std::max(k.smem, std::max(h->cx.smem, h->cy.smem));
+		}
+		members[c].push_back(i);
+	}
+	// blocks of the largest problems first, so the tail of a launch is short
+	auto work = [&](int i) { return (long long)b->h[i]->Nx * b->h[i]->Ny * b->h[i]->U; };
+	std::vector<int> xp, xl, yp, yl;
+	for (size_t c = 0; c < b->cls.size(); c++) {
+		BatchClass& k = b->cls[c];
+		std::vector<int>& m = members[c];
+		std::stable_sort(m.begin(), m.end(), [&](int a, int d) { return work(a) > work(d); });
+		k.xoff = (int)xp.size();
+		k.yoff = (int)yp.size();
+		for (int i : m) {
+			const pfcg_handle* h = b->h[i];
+			const int gx = k.ct ? h->cxs.grid : h->cx.grid, gy = k.ct ? h->cys.grid : h->cy.grid;
+			for (int t = 0; t < gx; t++) { xp.push_back(i); xl.push_back(t); }
+			for (int g = 0; g < gy; g++) { yp.push_back(i); yl.push_back(g); }
+		}
+		k.xn = (int)xp.size() - k.xoff;
+		k.yn = (int)yp.size() - k.yoff;
+		cudaError_t e = cudaStreamCreateWithFlags(&k.stream, cudaStreamNonBlocking);
+		if (e == cudaSuccess) e = cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming);
+		// the kernels' shared-memory limits are set here, outside any capture
+		for (int pass = 0; pass < 2 && e == cudaSuccess; pass++)
+			e = k.ct ? launch_ct_batch<T>(pass, k.U, k.N, nullptr, nullptr, nullptr, 0, pass ? k.cy : k.cx, k.stream)
+			         : launch_generic_batch<T>(pass, nullptr, nullptr, nullptr, 0, k.threads, k.smem, k.stream);
+		if (e != cudaSuccess) return bfail(e, "batch class");
 	}
 	b->xblocks = (int)xp.size();
 	b->yblocks = (int)yp.size();
-	pfcg_handle* h0 = b->h[0];
-	auto bfail = [&](cudaError_t e, const char* what) {
-		b->err = std::string(what) + ": " + cudaGetErrorString(e);
-		return PFCG_ECUDA;
-	};
-	cudaError_t e;
+	cudaError_t e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+	if (e != cudaSuccess) return bfail(e, "cudaEventCreate");
 	if ((e = cudaMalloc(&b->d_xargs, sizeof(XArgs<T>) * n)) != cudaSuccess) return bfail(e, "cudaMalloc");
 	if ((e = cudaMalloc(&b->d_yargs, sizeof(YArgs<T>) * n)) != cudaSuccess) return bfail(e, "cudaMalloc");
 	if ((e = cudaMalloc(&b->d_blk, sizeof(int) * (2 * xp.size() + 2 * yp.size()))) != cudaSuccess) return bfail(e, "cudaMalloc");
@@ -1231,23 +1298,38 @@ template <typename T> int batch_build(pfcg_batch* b) {
 	if ((e = cudaMemcpy(q + 2 * xp.size() + yp.size(), yl.data(), sizeof(int) * yl.size(), cudaMemcpyHostToDevice)) !=
 	    cudaSuccess)
 		return bfail(e, "cudaMemcpy");
-	(void)h0;
 	return 0;
 }
 
+// nsteps steps of every class, each class a chain on its own stream forked
+// from and joined back into the batch stream (which is capturing a graph).
 template <typename T> int batch_launch_steps(pfcg_batch* b, int nsteps) {
 	const int* q = b->d_blk;
 	const int* xp = q;
 	const int* xl = q + b->xblocks;
 	const int* yp = q + 2 * b->xblocks;
 	const int* yl = yp + b->yblocks;
-	for (int s = 0; s < nsteps; s++) {
-		cudaError_t e = launch_batch_step<T>((const XArgs<T>*)b->d_xargs, (const YArgs<T>*)b->d_yargs, xp, xl, b->xblocks, yp,
-		                                     yl, b->yblocks, b->threads, b->smem, b->stream);
-		if (e != cudaSuccess) {
-			b->err = std::string("batch step: ") + cudaGetErrorString(e);
-			return PFCG_ECUDA;
+	cudaError_t e = cudaEventRecord(b->fork, b->stream);
+	for (BatchClass& k : b->cls) {
+		if (e == cudaSuccess) e = cudaStreamWaitEvent(k.stream, b->fork, 0);
+		for (int s = 0; s < nsteps && e == cudaSuccess; s++) {
+			if (k.ct) {
+				e = launch_ct_batch<T>(0, k.U, k.N, b->d_xargs, xp + k.xoff, xl + k.xoff, k.xn, k.cx, k.stream);
+				if (e == cudaSuccess)
+					e = launch_ct_batch<T>(1, k.U, k.N, b->d_yargs, yp + k.yoff, yl + k.yoff, k.yn, k.cy, k.stream);
+			} else {
+				e = launch_generic_batch<T>(0, b->d_xargs, xp + k.xoff, xl + k.xoff, k.xn, k.threads, k.smem, k.stream);
+				if (e == cudaSuccess)
+					e = launch_generic_batch<T>(1, b->d_yargs, yp + k.yoff, yl + k.yoff, k.yn, k.threads, k.smem, k.stream);
+			}
 		}
+		// joined even after an error, so that the capture can end
+		cudaEventRecord(k.done, k.stream);
+		cudaStreamWaitEvent(b->stream, k.done, 0);
+	}
+	if (e != cudaSuccess) {
+		b->err = std::string("batch step: ") + cudaGetErrorString(e);
+		return PFCG_ECUDA;
 	}
 	return 0;
 }
@@ -1272,7 +1354,9 @@ int pfcg_batch_create(int nprob, const pfcg_params* params, const int* Nx, const
 		const int rc = pfcg_create(&params[i], Nx[i], Ny[i], dx[i], dy[i], prec, &h);
 		if (rc) return bail(rc);
 		b->h.push_back(h);
-		// the batch runs the runtime-plan kernels for every size
+		// sizes with specialised kernels run them in their fixed shape; the
+		// others run the runtime-plan kernels, in the shape the autotuner picks
+		if (batch_ct(h)) continue;
 		h->cxs = h->cx;
 		h->cys = h->cy;
 		if (autotune) {
@@ -1308,8 +1392,6 @@ int pfcg_batch_step(pfcg_batch* b, int nsteps) {
 	// every problem's own stream must be idle (uploads are synchronous)
 	auto it = b->graphs.find(nsteps);
 	if (it == b->graphs.end()) {
-		if (b->prec == PFCG_FP64) prepare_batch_kernels<double>();
-		else prepare_batch_kernels<float>();
 		cudaGraph_t g;
 		cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
 		if (e != cudaSuccess) { b->err = cudaGetErrorString(e); g_err = b->err; return PFCG_ECUDA; }
@@ -1339,7 +1421,7 @@ int pfcg_batch_step(pfcg_batch* b, int nsteps) {
 
 int pfcg_batch_launches(const pfcg_batch* b, int nsteps, long long* kernels, long long* graph_launches) {
 	if (!b) return PFCG_EARG;
-	if (kernels) *kernels = 2LL * nsteps;
+	if (kernels) *kernels = 2LL * nsteps * (long long)b->cls.size();
 	if (graph_launches) *graph_launches = 1;
 	return 0;
 }
@@ -1349,6 +1431,11 @@ void pfcg_batch_destroy(pfcg_batch* b) {
 	if (b->stream) cudaStreamSynchronize(b->stream);
 	for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
 	for (pfcg_handle* h : b->h) pfcg_destroy(h);
+	for (BatchClass& k : b->cls) {
+		if (k.stream) cudaStreamDestroy(k.stream);
+		if (k.done) cudaEventDestroy(k.done);
+	}
+	if (b->fork) cudaEventDestroy(b->fork);
 	cudaFree(b->d_xargs);
 	cudaFree(b->d_yargs);
 	cudaFree(b->d_blk);

@@ -126,13 +126,20 @@ int spec_twiddles(bool fp64, int N);
 template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
 template <typename T> cudaError_t launch_ypass(int mode, const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s);
 
-// One step of many problems: the batched x-pass and y-pass kernels over
-// per-problem arguments in device memory and per-block (problem, tile) tables.
+// One batched STEP pass (pass 0 = x, 1 = y) over per-problem arguments in
+// device memory (XArgs<T> or YArgs<T> array) and per-block (problem, tile or
+// column group) tables of nblk blocks. launch_ct_batch: every block's problem
+// has U fields and length N, which has specialised kernels (launch shape c of
+// those problems); launch_generic_batch: the runtime-plan kernels, any sizes.
+// nblk = 0 only prepares the kernels' shared-memory limits (call it before
+// capturing a graph).
 template <typename T> void prepare_batch_kernels();
 template <typename T>
-cudaError_t launch_batch_step(const XArgs<T>* xprobs, const YArgs<T>* yprobs, const int* xblk_prob, const int* xblk_local,
-                              int xblocks, const int* yblk_prob, const int* yblk_local, int yblocks, int threads, int smem,
-                              cudaStream_t s);
+cudaError_t launch_ct_batch(int pass, int U, int N, const void* probs, const int* bp, const int* bl, int nblk,
+                            const LaunchCfg& c, cudaStream_t s);
+template <typename T>
+cudaError_t launch_generic_batch(int pass, const void* probs, const int* bp, const int* bl, int nblk, int threads,
+                                 int smem, cudaStream_t s);
 
 // Parseval sums for up to MAX_TRIAL box sizes (see kernels.cu): out[t] += ...
 template <typename T>

@@ -8,8 +8,9 @@ template cudaError_t launch_ypass<double>(int, const YArgs<double>&, const Launc
 template cudaError_t launch_kspace_energy<double>(const cplx<double>*, long long, const Model&, const Geom&, int, const double*,
                                                const double*, double*, cudaStream_t);
 
-template cudaError_t launch_batch_step<double>(const XArgs<double>*, const YArgs<double>*, const int*, const int*, int, const int*,
-                                            const int*, int, int, int, cudaStream_t);
+template cudaError_t launch_ct_batch<double>(int, int, int, const void*, const int*, const int*, int, const LaunchCfg&,
+                                           cudaStream_t);
+template cudaError_t launch_generic_batch<double>(int, const void*, const int*, const int*, int, int, int, cudaStream_t);
 
 template void prepare_batch_kernels<double>();
 

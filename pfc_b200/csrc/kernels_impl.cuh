@@ -1121,6 +1121,23 @@ __global__ void __launch_bounds__(MAXNT, 1)
 }
 
 // Raises the dynamic shared-memory limit of a kernel once per device.
+// Batched STEP passes of the kernels specialised on a length: every block of
+// the launch belongs to a problem of that length and field count (one launch
+// per such class of a batch), so the body is the single-problem one.
+template <typename T, int U, int MODE, int NC, int RC>
+__global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MINB)
+    xpass_ct_batch_kernel(const XArgs<T>* __restrict__ probs, const int* __restrict__ blk_prob,
+                          const int* __restrict__ blk_local) {
+	xpass_body<T, U, MODE, NC, RC>(probs[blk_prob[blockIdx.x]], blk_local[blockIdx.x]);
+}
+
+template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK>
+__global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC, FUSEDK>::NT, YCfg<T, U, NC, CCC, RC, FUSEDK>::MINB)
+    ypass_ct_batch_kernel(const YArgs<T>* __restrict__ probs, const int* __restrict__ blk_prob,
+                          const int* __restrict__ blk_local) {
+	ypass_body<T, U, MODE, NC, CCC, RC, FUSEDK>(probs[blk_prob[blockIdx.x]], blk_local[blockIdx.x]);
+}
+
 template <typename K> static void smem_attr(K k, unsigned long long& mask) {
 	int dev = 0;
 	cudaGetDevice(&dev);
@@ -1222,12 +1239,42 @@ template <typename T, int U, int N> cudaError_t ct_ystep(const YArgs<T>& a, cons
 	return ylaunch<T, U, YP_STEP, N, Spec<T>::ycc(U, N), Spec<T>::xr(U, N)>(a, c, s);
 }
 
+// Batched STEP passes over nblk blocks of problems of length N (nblk = 0 only
+// sets the kernel's shared-memory limit, which must not happen under capture).
+template <typename T, int U, int N>
+cudaError_t ct_xbatch(const XArgs<T>* probs, const int* bp, const int* bl, int nblk, const LaunchCfg& c, cudaStream_t s) {
+	auto k = xpass_ct_batch_kernel<T, U, XP_STEP, N, Spec<T>::xr(U, N)>;
+	static unsigned long long mask = 0;
+	smem_attr(k, mask);
+	if (nblk > 0) k<<<nblk, c.block, c.smem, s>>>(probs, bp, bl);
+	return cudaGetLastError();
+}
+template <typename T, int U, int N>
+cudaError_t ct_ybatch(const YArgs<T>* probs, const int* bp, const int* bl, int nblk, const LaunchCfg& c, cudaStream_t s) {
+	constexpr int CC = Spec<T>::ycc(U, N), R = Spec<T>::xr(U, N);
+	static unsigned long long m1 = 0, m2 = 0;
+	if (c.spec == 2) {
+		auto k = ypass_ct_batch_kernel<T, U, YP_STEP, N, CC, R, false>;
+		smem_attr(k, m2);
+		if (nblk > 0) k<<<nblk, c.block, c.smem, s>>>(probs, bp, bl);
+	} else {
+		auto k = ypass_ct_batch_kernel<T, U, YP_STEP, N, CC, R, true>;
+		smem_attr(k, m1);
+		if (nblk > 0) k<<<nblk, c.block, c.smem, s>>>(probs, bp, bl);
+	}
+	return cudaGetLastError();
+}
+
 #ifndef PFCG_CT_TU
 #define PFCG_CT_TU 0
 #endif
 #define PFCG_CT_DECL(EXT, U, N)                                                                                        \
 	EXT template cudaError_t ct_xstep<float, U, N>(const XArgs<float>&, const LaunchCfg&, cudaStream_t);               \
-	EXT template cudaError_t ct_ystep<float, U, N>(const YArgs<float>&, const LaunchCfg&, cudaStream_t);
+	EXT template cudaError_t ct_ystep<float, U, N>(const YArgs<float>&, const LaunchCfg&, cudaStream_t);               \
+	EXT template cudaError_t ct_xbatch<float, U, N>(const XArgs<float>*, const int*, const int*, int, const LaunchCfg&,  \
+	                                                cudaStream_t);                                                     \
+	EXT template cudaError_t ct_ybatch<float, U, N>(const YArgs<float>*, const int*, const int*, int, const LaunchCfg&,  \
+	                                                cudaStream_t);
 #if PFCG_CT_TU != 256
 PFCG_CT_DECL(extern, 1, 256)
 PFCG_CT_DECL(extern, 2, 256)
@@ -1280,6 +1327,49 @@ template <typename T, int U> static cudaError_t ct_ydispatch(const YArgs<T>& a, 
 		}
 	}
 	return cudaErrorInvalidValue;
+}
+
+// One launch of the batched STEP pass (pass 0 = x, 1 = y) of the class of
+// problems with U fields and length N; cudaErrorInvalidValue where the size
+// has no specialised kernel.
+template <typename T, int U>
+static cudaError_t ct_batch_u(int pass, int N, const void* probs, const int* bp, const int* bl, int nblk,
+                              const LaunchCfg& c, cudaStream_t s) {
+#define PFCG_CT_CASE(NN)                                                                                              \
+	case NN:                                                                                                           \
+		return pass == 0 ? ct_xbatch<T, U, NN>((const XArgs<T>*)probs, bp, bl, nblk, c, s)                            \
+		                 : ct_ybatch<T, U, NN>((const YArgs<T>*)probs, bp, bl, nblk, c, s);
+	switch (N) {
+		PFCG_CT_CASE(4096)
+		PFCG_CT_CASE(2048)
+	}
+	if constexpr (std::is_same<T, float>::value) {
+		switch (N) {
+			PFCG_CT_CASE(1536)
+			PFCG_CT_CASE(1024)
+			PFCG_CT_CASE(768)
+			PFCG_CT_CASE(512)
+			PFCG_CT_CASE(256)
+		}
+	}
+#undef PFCG_CT_CASE
+	return cudaErrorInvalidValue;
+}
+template <typename T>
+cudaError_t launch_ct_batch(int pass, int U, int N, const void* probs, const int* bp, const int* bl, int nblk,
+                            const LaunchCfg& c, cudaStream_t s) {
+	if (U == 1) return ct_batch_u<T, 1>(pass, N, probs, bp, bl, nblk, c, s);
+	if (U == 2) return ct_batch_u<T, 2>(pass, N, probs, bp, bl, nblk, c, s);
+	return cudaErrorInvalidValue;
+}
+template <typename T>
+cudaError_t launch_generic_batch(int pass, const void* probs, const int* bp, const int* bl, int nblk, int threads,
+                                 int smem, cudaStream_t s) {
+	prepare_batch_kernels<T>();
+	if (nblk <= 0) return cudaGetLastError();
+	if (pass == 0) xpass_batch_kernel<T><<<nblk, threads, smem, s>>>((const XArgs<T>*)probs, bp, bl);
+	else ypass_batch_kernel<T><<<nblk, threads, smem, s>>>((const YArgs<T>*)probs, bp, bl);
+	return cudaGetLastError();
 }
 
 template <typename T, int U> static cudaError_t xlaunch_mode(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
@@ -1336,18 +1426,6 @@ template <typename T> void prepare_batch_kernels() {
 	static unsigned long long mx = 0, my = 0;
 	smem_attr(xpass_batch_kernel<T>, mx);
 	smem_attr(ypass_batch_kernel<T>, my);
-}
-
-template <typename T>
-cudaError_t launch_batch_step(const XArgs<T>* xprobs, const YArgs<T>* yprobs, const int* xblk_prob, const int* xblk_local,
-                              int xblocks, const int* yblk_prob, const int* yblk_local, int yblocks, int threads, int smem,
-                              cudaStream_t s) {
-	prepare_batch_kernels<T>();
-	xpass_batch_kernel<T><<<xblocks, threads, smem, s>>>(xprobs, xblk_prob, xblk_local);
-	cudaError_t e = cudaGetLastError();
-	if (e != cudaSuccess) return e;
-	ypass_batch_kernel<T><<<yblocks, threads, smem, s>>>(yprobs, yblk_prob, yblk_local);
-	return cudaGetLastError();
 }
 
 template <typename T>

@@ -367,7 +367,8 @@ class _Problem(Relaxation):
 
 class Batch:
     """Many relaxations stepped together (pfcg_batch_*): one CUDA graph per step
-    count, two batched kernels per step."""
+    count; per step, two batched kernels for each class of problems (one class
+    per size and field count with specialised kernels, one for the rest)."""
 
     def __init__(self, problems, precision: str = "fp32", autotune: bool = True):
         """problems: list of (Params, Nx, Ny, dx, dy)."""
@@ -392,6 +393,14 @@ class Batch:
         if rc:
             raise PfcError(rc, self.L.pfcg_last_error(None).decode())
         return rc
+
+    def launches(self, nsteps: int = 1):
+        """(kernel launches, graph launches) of pfcg_batch_step(nsteps)."""
+        k, g = ctypes.c_longlong(), ctypes.c_longlong()
+        rc = self.L.pfcg_batch_launches(self.b, nsteps, ctypes.byref(k), ctypes.byref(g))
+        if rc:
+            raise PfcError(rc, self.L.pfcg_last_error(None).decode())
+        return k.value, g.value
 
     def close(self):
         if getattr(self, "b", None):

@@ -13,12 +13,15 @@ pytestmark = pytest.mark.gpu
 
 
 def problems():
-    """Mixed sizes (radix 2, 3, 5), one and two fields, and box-size scalings of one state."""
+    """Mixed sizes (radix 2, 3, 5), one and two fields, and box-size scalings of one
+    state. 256 (twice), 512 and 768 have specialised kernels (a class of their
+    own each in the batch, 768 with a radix-3 tail pass); the rest run the
+    runtime-plan kernels together."""
     out = []
     p1 = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
     p2 = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
     base = synth.noise_state(96, 96, 0.25, 0.05, 40)[None]
-    for k, (N, U) in enumerate([(256, 1), (96, 2), (160, 1), (384, 2), (128, 1)]):
+    for k, (N, U) in enumerate([(256, 1), (96, 2), (160, 1), (384, 2), (128, 1), (512, 2), (768, 1), (256, 1)]):
         if U == 1:
             f = synth.noise_state(N, N, 0.25, 0.05, 50 + k)[None]
             out.append((p1, N, N, math.pi / 4, math.pi / 4, f))
@@ -38,6 +41,8 @@ def test_batch_matches_single_problems(precision, tol):
             prob.upload(p[5])
         b.step(7)
         b.step(13)  # a second captured graph
+        # FP32: classes (1, 256), (2, 512), (1, 768) and the runtime-plan rest
+        assert b.launches(7) == (2 * 7 * (4 if precision == "fp32" else 1), 1)
         got = [prob.download() for prob in b.problems]
         energies = [prob.evaluate()[0] for prob in b.problems]
     for p, g, e in zip(probs, got, energies):
