@@ -196,8 +196,9 @@ def batch_problems(seed: int = 7, n: int = 96):
 
 def run_batch(args):
     """Config C4: aggregate grid-point updates/s of the batched launch (two
-    kernels per step for all problems, steps captured in one CUDA graph) against
-    the same problems relaxed one after another through their own handles."""
+    kernels per step for each class of problems of one size and field count,
+    the classes side by side, steps captured in one CUDA graph) against the
+    same problems relaxed one after another through their own handles."""
     import torch
 
     probs = batch_problems()
