@@ -847,10 +847,10 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 		// model constants in the transform precision, once per CTA
 		const StepConsts<T, U> K(a.m, Nx, Ny);
 		const T dkxT = (T)a.g.dkx, dkyT = (T)a.g.dky;
-		// update of one (kx, ky) entry for all fields, pfc-relax.c:1215-1244
-		auto update = [&](int c, int kx, int ky, const cplx<T>(&Nv)[U]) {
-			T A[U], Bn[U], cu[npairs<T, U>()];
-			entry_coef<T, U>(K, step_k2<T>(kx, ky, Ny, dkxT, dkyT, a.g), A, Bn, cu);
+		// update of one (kx, ky) entry for all fields with its coefficients
+		// (A, B, couplings of k^2), pfc-relax.c:1215-1244
+		auto apply = [&](int c, int kx, int ky, const cplx<T>(&Nv)[U], const T(&A)[U], const T(&Bn)[U],
+		                 const T(&cu)[npairs<T, U>()]) {
 			cplx<T> Mv[U];
 #pragma unroll
 			for (int u = 0; u < U; u++) Mv[u] = cscale(sm[(u * CC + c) * ld + pad<T>(ky)], K.invN);
@@ -873,7 +873,45 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 				sm[(u * CC + c) * ld + pad<T>(ky)] = nn;
 			}
 		};
-		if constexpr (C::CT && (CCC * NC) % C::NT == 0) {
+		auto update = [&](int c, int kx, int ky, const cplx<T>(&Nv)[U]) {
+			T A[U], Bn[U], cu[npairs<T, U>()];
+			entry_coef<T, U>(K, step_k2<T>(kx, ky, Ny, dkxT, dkyT, a.g), A, Bn, cu);
+			apply(c, kx, ky, Nv, A, Bn, cu);
+		};
+		if constexpr (C::CT && (CCC * NC / 2) % C::NT == 0) {
+			// entries ky and NC - ky have the same k^2 (signed wave numbers ky and
+			// -ky), so each thread takes such pairs and evaluates the coefficients
+			// once for both; ky = 0 is paired with the self-mirrored NC / 2 and
+			// evaluates them twice
+			constexpr int HALF = NC / 2;
+			constexpr int PH = CCC * HALF / C::NT;
+			cplx<T> Nv[PH][2][U];
+#pragma unroll
+			for (int i = 0; i < PH; i++) {
+				const int h = tid + i * C::NT;
+				const int c = h / HALF, kb = h % HALF;
+				const int ky2 = kb ? NC - kb : HALF;
+				const long long col = (long long)(kx0 + c) * NC;
+#pragma unroll
+				for (int u = 0; u < U; u++) {
+					Nv[i][0][u] = (c < ncol) ? a.spec[u * a.sstride + col + kb] : mk<T>((T)0, (T)0);
+					Nv[i][1][u] = (c < ncol) ? a.spec[u * a.sstride + col + ky2] : mk<T>((T)0, (T)0);
+				}
+			}
+#pragma unroll
+			for (int i = 0; i < PH; i++) {
+				const int h = tid + i * C::NT;
+				const int c = h / HALF, kb = h % HALF;
+				const int kx = kx0 + c;
+				if (c < ncol) {
+					T A[U], Bn[U], cu[npairs<T, U>()];
+					entry_coef<T, U>(K, step_k2<T>(kx, kb, NC, dkxT, dkyT, a.g), A, Bn, cu);
+					apply(c, kx, kb, Nv[i][0], A, Bn, cu);
+					if (kb == 0) entry_coef<T, U>(K, step_k2<T>(kx, HALF, NC, dkxT, dkyT, a.g), A, Bn, cu);
+					apply(c, kx, kb ? NC - kb : HALF, Nv[i][1], A, Bn, cu);
+				}
+			}
+		} else if constexpr (C::CT && (CCC * NC) % C::NT == 0) {
 			// every thread owns PER entries: issue all spectral-state loads first
 			constexpr int PER = CCC * NC / C::NT;
 			cplx<T> Nv[PER][U];
