@@ -241,6 +241,36 @@ def test_specialised_fp32_lengths_match_oracle(U, N, monkeypatch):
     assert not np.array_equal(got["0"], got["1"])
 
 
+@pytest.mark.parametrize("U,Nx,Ny", [(2, 1024, 512), (1, 768, 1536), (2, 256, 4096), (1, 1536, 256)])
+def test_specialised_fp32_rectangles_match_oracle(U, Nx, Ny):
+    """Rectangular grids whose x and y lengths both have specialised kernels:
+    the x-pass takes Nx's row tile, and the y-pass is specialised only where
+    Ny's kernels use the same tile (1024 x 512, 768 x 1536, 1536 x 256), else
+    the runtime-plan y-pass reads that layout (256 x 4096 at U = 2)."""
+    dx, dy = 0.7, 0.75
+    steps = 5
+    if U == 1:
+        p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+        f0 = synth.noise_state(Nx, Ny, 0.25, 0.05, 33)[None]
+    else:
+        p = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
+        f0 = synth.stripes2(Nx, Ny, dx, dy, max(Nx // 8, 8), (0.3, -0.3), (0.3, 0.3), (7.2552, 7.2552 * 1.04), 0.02,
+                            34)
+    o = pyoracle.Oracle(p, Nx, Ny, dx, dy)
+    o.upload(f0)
+    o.step(steps)
+    ref = o.download()
+    fo, _ = o.evaluate()
+    o.close()
+    with lib.Relaxation(p, Nx, Ny, dx, dy, "fp32") as r:
+        r.upload(f0)
+        r.step(steps)
+        got = r.download()
+        fg, _ = r.evaluate()
+    assert np.abs(got - ref).max() < 2e-5, np.abs(got - ref).max()
+    assert rel(fg, fo) < 1e-6, rel(fg, fo)
+
+
 @pytest.mark.parametrize("U,Nx,Ny", [(1, 8192, 8), (2, 8, 8192), (1, 7000, 12), (2, 10, 6174), (1, 8192, 40),
                                       (2, 7168, 8)])
 def test_extreme_shapes_match_oracle(U, Nx, Ny):
