@@ -191,7 +191,7 @@ int pfcg_profile_read(pfcg_handle* h, double* ms, long long* launches, int nkind
  * steps each and keeps the fastest; results are cached per (precision, U, Nx,
  * Ny) for the process. Call before pfcg_upload: the timing steps run on the
  * handle's buffers, which are cleared afterwards. Sizes with compile-time
- * specialised kernels (FP32: 256, 512, 768, 1024, 1536, 2048, 4096; FP64: 2048,
+ * specialised kernels (FP32: 256, 384, 512, 768, 1024, 1536, 2048, 4096; FP64: 2048,
  * 4096) keep their fixed shape. No counterpart in
  * the reference (FFTW_MEASURE planning, pfc-relax.c:227-231, is the nearest). */
 int pfcg_autotune(pfcg_handle* h, int nsteps);

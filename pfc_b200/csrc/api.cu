@@ -815,11 +815,11 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	rc = fp64 ? upload_twiddles<double>(h, Nx, &h->twx) : upload_twiddles<float>(h, Nx, &h->twx);
 	if (!rc) rc = fp64 ? upload_twiddles<double>(h, Ny, &h->twy) : upload_twiddles<float>(h, Ny, &h->twy);
 	if (!rc && h->cxs.spec)
-		rc = fp64 ? upload_ct_twiddles<double>(h, Nx, ct_radix(true), &h->twctx)
-		          : upload_ct_twiddles<float>(h, Nx, ct_radix(false), &h->twctx);
+		rc = fp64 ? upload_ct_twiddles<double>(h, Nx, ct_radix(true, Nx), &h->twctx)
+		          : upload_ct_twiddles<float>(h, Nx, ct_radix(false, Nx), &h->twctx);
 	if (!rc && h->cys.spec)
-		rc = fp64 ? upload_ct_twiddles<double>(h, Ny, ct_radix(true), &h->twcty)
-		          : upload_ct_twiddles<float>(h, Ny, ct_radix(false), &h->twcty);
+		rc = fp64 ? upload_ct_twiddles<double>(h, Ny, ct_radix(true, Ny), &h->twcty)
+		          : upload_ct_twiddles<float>(h, Ny, ct_radix(false, Ny), &h->twcty);
 	if (rc) return bail(rc);
 	*out = h;
 	return 0;

@@ -164,9 +164,9 @@ cudaError_t launch_fields_gradpow(const double* g4, long long n, double power, d
 cudaError_t launch_scaled_acc(double* acc, const double* r, long long n, double* part, int nparts, cudaStream_t st);
 
 // elements per thread and main radix of the runtime-plan kernels; main radix
-// of the compile-time specialised ones
+// of the kernels specialised on the length N
 int max_elems_per_thread(bool fp64);
 int max_radix(bool fp64);
-int ct_radix(bool fp64);
+int ct_radix(bool fp64, int N);
 
 } // namespace pfcg

@@ -5,7 +5,7 @@ namespace pfcg {
 
 int max_elems_per_thread(bool fp64) { (void)fp64; return RT_MAXE; }
 int max_radix(bool fp64) { (void)fp64; return RT_MAXE; }
-int ct_radix(bool fp64) { return fp64 ? FftCfg<double>::MAXE : FftCfg<float>::MAXE; }
+int ct_radix(bool fp64, int N) { return fp64 ? ct_maxe<double>(N) : ct_maxe<float>(N); }
 
 // 0 where the size has no specialised kernel (Spec in kernels_impl.cuh)
 int spec_rows(bool fp64, int U, int N) { return fp64 ? Spec<double>::xr(U, N) : Spec<float>::xr(U, N); }
@@ -19,6 +19,7 @@ template <typename T> static int ct_twn(int N) {
 	}
 	if constexpr (M == 16) {
 		switch (N) {
+		case 384: return CtPlan<384, ct_maxe<T>(384)>::TWN;
 		case 1536: return CtPlan<1536, M>::TWN;
 		case 1024: return CtPlan<1024, M>::TWN;
 		case 768: return CtPlan<768, M>::TWN;
@@ -31,14 +32,14 @@ template <typename T> static int ct_twn(int N) {
 int spec_twiddles(bool fp64, int N) { return fp64 ? ct_twn<double>(N) : ct_twn<float>(N); }
 
 int spec_x_threads(bool fp64, int U, int N) {
-	const int maxe = ct_radix(fp64);
+	const int maxe = ct_radix(fp64, N);
 	const int P = (U * spec_rows(fp64, U, N) + 1) / 2;
 	return P * N / maxe <= MAXNT ? P * N / maxe : MAXNT;
 }
 int spec_y_threads(bool fp64, int U, int N, bool fused) {
 	// fused y-pass: one thread per (field, column, butterfly); otherwise as many
 	// sequences per FFT call as fit MAXNT threads
-	const int maxe = ct_radix(fp64);
+	const int maxe = ct_radix(fp64, N);
 	const int S = U * spec_cols(fp64, U, N);
 	if (fused && U <= 2 && S * N / maxe <= MAXNT) return S * N / maxe;
 	if (S * N / maxe <= MAXNT) return S * N / maxe;

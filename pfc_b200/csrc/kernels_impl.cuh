@@ -29,6 +29,12 @@ namespace pfcg {
 template <typename T> struct FftCfg;
 template <> struct FftCfg<float> { static constexpr int MAXE = 16; };
 template <> struct FftCfg<double> { static constexpr int MAXE = 8; };
+// Main radix (elements per thread) of the kernels specialised on the length N:
+// FftCfg's, except FP32 384 = 8 * 6 * 8, which has no radix-16 form with
+// radix-16 first and last passes.
+template <typename T> __host__ __device__ constexpr int ct_maxe(int N) {
+	return (sizeof(T) == 4 && N == 384) ? 8 : FftCfg<T>::MAXE;
+}
 // and of the runtime-plan kernels, in both precisions: 16 elements per thread
 // let 512 threads hold one 8192-point sequence (and 7168 / 7680 with a factor 7 / 5)
 constexpr int RT_MAXE = 16;
@@ -112,7 +118,7 @@ __device__ __forceinline__ float phi1f(float x, float A) {
 // runtime length and plan). P / S resident sequences, NSUB per FFT call, NT threads.
 template <typename T, int U, int NC, int RC> struct XCfg {
 	static constexpr bool CT = NC > 0;
-	static constexpr int MAXE = CT ? FftCfg<T>::MAXE : RT_MAXE;
+	static constexpr int MAXE = CT ? ct_maxe<T>(NC) : RT_MAXE;
 	static constexpr int P = CT ? (U * RC + 1) / 2 : 1;
 	static constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
 	static constexpr int NSUB = CT ? (P * NC / MAXE <= MAXNT ? P : MAXNT * MAXE / NC) : 1;
@@ -123,7 +129,7 @@ template <typename T, int U, int NC, int RC> struct XCfg {
 
 template <typename T, int U, int NC, int CCC, int RC, bool FUSEDK = true> struct YCfg {
 	static constexpr bool CT = NC > 0;
-	static constexpr int MAXE = CT ? FftCfg<T>::MAXE : RT_MAXE;
+	static constexpr int MAXE = CT ? ct_maxe<T>(NC) : RT_MAXE;
 	static constexpr int S = CT ? U * CCC : 1;
 	static constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
 	static constexpr bool FUSED = FUSEDK && CT && CtPlan<(CT ? NC : 256), MAXE>::FUSABLE && U <= 2 &&
@@ -1236,15 +1242,16 @@ template <typename T> struct Spec;
 // Rows per x-pass tile (xr) and columns per y-pass group (ycc) of the kernels
 // specialised on a compile-time length N, 0 where there is none. The row tile
 // is also the layout of `work` for the runtime-plan modes (evaluate, c2r, r2c),
-// so U * xr stays within MAX_CH: an FP32 x-pass CTA runs U * xr * N / 32
-// threads (512 at N = 4096 and 2048, N / 4 below). A y-pass CTA runs
-// U * ycc * N / 16 threads: 512, or 384 at N = 768 and 1536 (16^2 * 3, 16^2 * 6).
+// so U * xr stays within MAX_CH: an FP32 x-pass CTA runs U * xr * N / (2 M)
+// threads for the main radix M = ct_maxe (512 at N = 4096 and 2048, N / 4
+// below with M = 16, 192 at N = 384). A y-pass CTA runs U * ycc * N / M
+// threads: 512, or 384 at N = 384, 768 and 1536 (8^2 * 6, 16^2 * 3, 16^2 * 6).
 template <> struct Spec<float> {
 	static constexpr int x1(int N) {
-		return N == 4096 ? 4 : (N == 2048 || N == 1536 || N == 1024 || N == 768 || N == 512 || N == 256) ? 8 : 0;
+		return N == 4096 ? 4 : (N == 2048 || N == 1536 || N == 1024 || N == 768 || N == 512 || N == 384 || N == 256) ? 8 : 0;
 	}
 	static constexpr int y1(int N) {
-		return N == 4096 ? 2 : N == 2048 || N == 1536 ? 4 : N == 1024 || N == 768 ? 8 : N == 512 ? 16 : N == 256 ? 32 : 0;
+		return N == 4096 ? 2 : N == 2048 || N == 1536 ? 4 : N == 1024 || N == 768 || N == 384 ? 8 : N == 512 ? 16 : N == 256 ? 32 : 0;
 	}
 	static constexpr int xr(int U, int N) { return U == 1 ? x1(N) : U == 2 ? x1(N) / 2 : 0; }
 	static constexpr int ycc(int U, int N) { return U == 1 ? y1(N) : U == 2 ? y1(N) / 2 : 0; }
@@ -1317,6 +1324,10 @@ cudaError_t ct_ybatch(const YArgs<T>* probs, const int* bp, const int* bl, int n
 PFCG_CT_DECL(extern, 1, 256)
 PFCG_CT_DECL(extern, 2, 256)
 #endif
+#if PFCG_CT_TU != 384
+PFCG_CT_DECL(extern, 1, 384)
+PFCG_CT_DECL(extern, 2, 384)
+#endif
 #if PFCG_CT_TU != 512
 PFCG_CT_DECL(extern, 1, 512)
 PFCG_CT_DECL(extern, 2, 512)
@@ -1345,6 +1356,7 @@ template <typename T, int U> static cudaError_t ct_xdispatch(const XArgs<T>& a, 
 		case 1024: return ct_xstep<T, U, 1024>(a, c, s);
 		case 768: return ct_xstep<T, U, 768>(a, c, s);
 		case 512: return ct_xstep<T, U, 512>(a, c, s);
+		case 384: return ct_xstep<T, U, 384>(a, c, s);
 		case 256: return ct_xstep<T, U, 256>(a, c, s);
 		}
 	}
@@ -1361,6 +1373,7 @@ template <typename T, int U> static cudaError_t ct_ydispatch(const YArgs<T>& a, 
 		case 1024: return ct_ystep<T, U, 1024>(a, c, s);
 		case 768: return ct_ystep<T, U, 768>(a, c, s);
 		case 512: return ct_ystep<T, U, 512>(a, c, s);
+		case 384: return ct_ystep<T, U, 384>(a, c, s);
 		case 256: return ct_ystep<T, U, 256>(a, c, s);
 		}
 	}
@@ -1387,6 +1400,7 @@ static cudaError_t ct_batch_u(int pass, int N, const void* probs, const int* bp,
 			PFCG_CT_CASE(1024)
 			PFCG_CT_CASE(768)
 			PFCG_CT_CASE(512)
+			PFCG_CT_CASE(384)
 			PFCG_CT_CASE(256)
 		}
 	}

@@ -56,7 +56,7 @@ int main() {
 	check_dft<8, -1>(); check_dft<8, 1>();
 	check_dft<16, -1>(); check_dft<16, 1>();
 	// FP32 (radix 16) and FP64 (radix 8) specialised lengths
-	check_plan<256, 16>(); check_plan<512, 16>(); check_plan<768, 16>(); check_plan<1024, 16>();
+	check_plan<256, 16>(); check_plan<384, 8>(); check_plan<512, 16>(); check_plan<768, 16>(); check_plan<1024, 16>();
 	check_plan<1536, 16>(); check_plan<2048, 16>(); check_plan<4096, 16>();
 	check_plan<2048, 8>(); check_plan<4096, 8>();
 	return failures ? 1 : 0;

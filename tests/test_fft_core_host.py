@@ -21,4 +21,4 @@ def test_dfts_and_plans_on_host(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert out.returncode == 0, out.stdout
     lines = out.stdout.strip().splitlines()
-    assert len(lines) == 25 and all(l.endswith("ok") for l in lines), out.stdout
+    assert len(lines) == 26 and all(l.endswith("ok") for l in lines), out.stdout

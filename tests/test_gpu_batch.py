@@ -14,9 +14,9 @@ pytestmark = pytest.mark.gpu
 
 def problems():
     """Mixed sizes (radix 2, 3, 5), one and two fields, and box-size scalings of one
-    state. 256 (twice), 512 and 768 have specialised kernels (a class of their
-    own each in the batch, 768 with a radix-3 tail pass); the rest run the
-    runtime-plan kernels together."""
+    state. 256 (twice), 384, 512 and 768 have specialised kernels in FP32 (a
+    class of their own each in the batch, 768 with a radix-3 tail pass, 384 in
+    radix 8); the rest run the runtime-plan kernels together."""
     out = []
     p1 = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
     p2 = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
@@ -41,8 +41,8 @@ def test_batch_matches_single_problems(precision, tol):
             prob.upload(p[5])
         b.step(7)
         b.step(13)  # a second captured graph
-        # FP32: classes (1, 256), (2, 512), (1, 768) and the runtime-plan rest
-        assert b.launches(7) == (2 * 7 * (4 if precision == "fp32" else 1), 1)
+        # FP32: classes (1, 256), (2, 384), (2, 512), (1, 768) and the runtime-plan rest
+        assert b.launches(7) == (2 * 7 * (5 if precision == "fp32" else 1), 1)
         got = [prob.download() for prob in b.problems]
         energies = [prob.evaluate()[0] for prob in b.problems]
     for p, g, e in zip(probs, got, energies):

@@ -207,10 +207,11 @@ def test_specialised_sizes_match_oracle(U, N, steps):
 
 
 @pytest.mark.parametrize("U", [1, 2])
-@pytest.mark.parametrize("N", [256, 512, 768, 1024, 1536])
+@pytest.mark.parametrize("N", [256, 384, 512, 768, 1024, 1536])
 def test_specialised_fp32_lengths_match_oracle(U, N, monkeypatch):
     """The FP32 STEP kernels specialised on the lengths below 2048 (radix 16 with
-    a tail pass of radix 1, 2, 3, 4 or 6) against the CPU oracle, beside the
+    a tail pass of radix 1, 2, 3, 4 or 6; 384 as radix 8, 6, 8) against the CPU
+    oracle, beside the
     runtime-plan kernels (PFCG_GENERIC_KERNELS=1) on the same state. The two
     FP32 results differ in rounding only, which shows that a different
     transform ran."""
