@@ -770,6 +770,17 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 		ypass_step_fused<T, U, NC, CCC, RC, C::S, C::NT, MAXE>(a, sm, tws, kx0, ncol, tid);
 		return;
 	}
+	if constexpr (MODE == YP_STEP && C::CT) {
+		// this group's spectral-state columns into L2 now, so that the update's
+		// loads after the forward transform find them there: one 128-byte line
+		// per prefetch, all inside the live columns
+		constexpr int LPC = NC * (int)sizeof(cplx<T>) / 128; // lines per column
+		for (int i = tid; i < U * ncol * LPC; i += C::NT) {
+			const int u = i / (ncol * LPC), rest = i % (ncol * LPC);
+			const char* line = reinterpret_cast<const char*>(a.spec + u * a.sstride + (long long)kx0 * NC) + rest * 128;
+			asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+		}
+	}
 
 	// Register ends (STEP, one butterfly per thread per pass): the forward
 	// transform's first pass takes its inputs straight from global memory and
