@@ -886,7 +886,10 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 			for (int u = 0; u < U; u++) {
 				cplx<T> nn = cadd(cscale(Nv[u], A[u]), cscale(Mv[u], Bn[u]));
 				if (origin) nn = mk<T>((T)0, (T)0);
-				a.spec[u * a.sstride + (long long)kx * Ny + ky] = nn;
+				// streaming (evict-first) accesses for the spectral state, read
+				// and written once per step, leave L2 to `work`, which the next
+				// pass reads back
+				__stcs(a.spec + u * a.sstride + (long long)kx * Ny + ky, nn);
 				sm[(u * CC + c) * ld + pad<T>(ky)] = nn;
 			}
 		};
@@ -911,8 +914,8 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 				const long long col = (long long)(kx0 + c) * NC;
 #pragma unroll
 				for (int u = 0; u < U; u++) {
-					Nv[i][0][u] = (c < ncol) ? a.spec[u * a.sstride + col + kb] : mk<T>((T)0, (T)0);
-					Nv[i][1][u] = (c < ncol) ? a.spec[u * a.sstride + col + ky2] : mk<T>((T)0, (T)0);
+					Nv[i][0][u] = (c < ncol) ? __ldcs(a.spec + u * a.sstride + col + kb) : mk<T>((T)0, (T)0);
+					Nv[i][1][u] = (c < ncol) ? __ldcs(a.spec + u * a.sstride + col + ky2) : mk<T>((T)0, (T)0);
 				}
 			}
 #pragma unroll
