@@ -299,8 +299,28 @@ template <typename T, int U> __device__ __forceinline__ void ypass_mean_update(c
 // registers -> + mean, NaN check, NL, FP64 sum of NL -> forward FFT from
 // registers -> unpack -> Z tile. U in {1, 2}; pair p holds row p (U = 2: the
 // two fields as real and imaginary part) or rows 2p, 2p + 1 (U = 1).
+// Per-pass twiddle table of a specialised kernel into shared memory: all of a
+// thread's loads first, then its stores, so that the table's L2 latency is paid
+// once (callers issue their own global loads before it).
+template <typename T, int TWN, int NT>
+__device__ __forceinline__ void copy_twiddles(cplx<T>* tws, const cplx<T>* __restrict__ src, int tid) {
+	constexpr int TPT = (TWN + NT - 1) / NT;
+	cplx<T> t[TPT];
+#pragma unroll
+	for (int j = 0; j < TPT; j++) {
+		const int i = tid + j * NT;
+		if (TWN % NT == 0 || i < TWN) t[j] = src[i];
+	}
+#pragma unroll
+	for (int j = 0; j < TPT; j++) {
+		const int i = tid + j * NT;
+		if (TWN % NT == 0 || i < TWN) tws[i] = t[j];
+	}
+}
+
 template <typename T, int U, int NC, int RC, int P, int NT, int MAXE>
-__device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm, const cplx<T>* tws, int tile, int tid) {
+__device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm, cplx<T>* tws, int tile, int tid,
+                                                 bool load_tw) {
 	using PL = CtPlan<NC, MAXE>;
 	using RB = RegBlock<NC, MAXE, P, NT, T>;
 	constexpr int LD = NC + (NC >> Pad<T>::SHIFT) + 1;
@@ -326,6 +346,7 @@ __device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm,
 			if (k > 0 && 2 * k < NC) sm[p * LD + pad<T>(NC - k)] = mk<T>(A.x + B.y, B.x - A.y);
 		}
 	}
+	if (load_tw) copy_twiddles<T, CtPlan<NC, MAXE>::TWN, NT>(tws, a.twct, tid);
 	__syncthreads();
 	// inverse transform: all passes but the last in shared memory, the last into registers
 	ct_pass<NC, PL::radix(0), PL::ns(0), PL::twoff(0), P, NT, +1, T>(sm, tws, tid);
@@ -547,13 +568,14 @@ __device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile, co
 	const int nt = C::CT ? C::NT : (int)blockDim.x;
 	const long long tofs = (long long)tile * H * R;
 	cplx<T>* tws = sm + (C::CT ? C::P * C::LD : 0);
-	if constexpr (C::CT) {
-		if (load_tw)
-			for (int i = tid; i < C::TWN; i += C::NT) tws[i] = a.twct[i];
+	constexpr bool XFUSED = MODE == XP_STEP && C::CT && CtPlan<(C::CT ? NC : 256), MAXE>::FUSABLE && C::NSUB == C::P &&
+	                        U <= 2 && (U * RC) % 2 == 0;
+	if constexpr (C::CT && !XFUSED) {
+		if (load_tw) copy_twiddles<T, C::TWN, C::NT>(tws, a.twct, tid);
 	}
-	if constexpr (MODE == XP_STEP && C::CT && CtPlan<NC, MAXE>::FUSABLE && C::NSUB == C::P && U <= 2 &&
-	              (U * RC) % 2 == 0) {
-		xpass_step_fused<T, U, NC, RC, C::P, C::NT, MAXE>(a, sm, tws, tile, tid);
+	if constexpr (XFUSED) {
+		// the fused pass copies the twiddles after issuing its tile loads
+		xpass_step_fused<T, U, NC, RC, C::P, C::NT, MAXE>(a, sm, tws, tile, tid, load_tw);
 		return;
 	}
 
@@ -761,6 +783,8 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 	const int tid = threadIdx.x;
 	const int nt = C::CT ? C::NT : (int)blockDim.x;
 	cplx<T>* tws = sm + (C::CT ? C::S * C::LD : 0);
+	// (copying the twiddles after the register-end loads instead, as the
+	// x-pass does, measured 2 % slower here)
 	if constexpr (C::CT) {
 		if (load_tw)
 			for (int i = tid; i < C::TWN; i += C::NT) tws[i] = a.twct[i];
