@@ -333,8 +333,6 @@ __device__ __forceinline__ void fft_batches(cplx<T>* buf, int ld, int S, int SB,
 // memory laid out [(r - 1) * Ns + jm] (consecutive threads read consecutive
 // words), entry = exp(-2 pi i r jm / (Ns R)).
 
-__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
-
 // N = RM^A * RT with RM^(A+1) not dividing N; RT (1 = none) is one of the
 // radices dft() has (2, 3, 4, 6, 8 for the lengths used). The tail radix, when
 // there is one, is pass 1 (second), so that the first and the last pass both
