@@ -48,7 +48,7 @@ def test_create_rejects_bad_arguments_without_gpu_work():
     (2048, 2048, 4, lib.FP64, 1), (30, 42, 3, lib.FP64, 1), (66, 64, 1, lib.FP32, 0), (64, 64, 0, lib.FP32, 0),
     (8192, 8192, 2, lib.FP32, 1), (8192, 8192, 2, lib.FP64, 0), (4096, 4096, 4, lib.FP32, 1),
     (1536, 1536, 2, lib.FP32, 1), (384, 384, 2, lib.FP32, 1), (998, 998, 1, lib.FP32, 0),  # 499 is prime
-    (1001, 1000, 1, lib.FP32, 0)])  # odd lengths have no half spectrum of the reference's layout
+    (1001, 1000, 1, lib.FP32, 0)])  # odd lengths are refused: even 8..8192 only
 def test_size_supported_for(Nx, Ny, U, prec, ok):
     """The exact host-side check of what pfcg_create accepts (no device work)."""
     assert lib.load().pfcg_size_supported_for(Nx, Ny, U, prec) == ok
