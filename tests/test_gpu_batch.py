@@ -71,3 +71,28 @@ def test_autotune_keeps_results(N):
             r.step(30)
             out.append(r.download())
     assert np.abs(out[0] - out[1]).max() < 1e-5
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-6)])
+def test_batch_specialised_2048(precision, tol):
+    """2048² problems (specialised in both precisions: a class of their own, in
+    FP64 on the same kernels as the persistent single-problem grid) beside a
+    runtime-plan one, against the same problems stepped one at a time."""
+    p1 = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+    p2 = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
+    probs = [(p1, 2048, 2048, math.pi / 4, math.pi / 4, synth.noise_state(2048, 2048, 0.25, 0.05, 80)[None]),
+             (p2, 2048, 2048, 0.7, 0.7,
+              synth.stripes2(2048, 2048, 0.7, 0.7, 256, (0.3, -0.3), (0.3, 0.3), (7.2552, 7.2552 * 1.04), 0.02, 81)),
+             (p1, 96, 96, math.pi / 4, math.pi / 4, synth.noise_state(96, 96, 0.25, 0.05, 82)[None])]
+    with lib.Batch([p[:5] for p in probs], precision, autotune=False) as b:
+        for prob, p in zip(b.problems, probs):
+            prob.upload(p[5])
+        b.step(4)
+        assert b.launches(4) == (2 * 4 * 3, 1)
+        got = [prob.download() for prob in b.problems]
+    for p, g in zip(probs, got):
+        with lib.Relaxation(*p[:5], precision) as r:
+            r.upload(p[5])
+            r.step(4)
+            ref = r.download()
+        assert np.abs(g - ref).max() < tol
