@@ -1,6 +1,8 @@
 // Kernels of the B200 relaxation path; see kernels.cuh for the data layout.
 // Included by kernels_f32.cu / kernels_f64.cu, which instantiate one precision
-// each, and by kernels_common.cu for the precision-independent parts.
+// each, by kernels_f32_<N>.cu, which instantiate the FP32 kernels specialised on
+// one length N below 2048, and by kernels_common.cu for the
+// precision-independent parts.
 //
 // Reference correspondence (demos/honey/pfc-relax.c):
 //   xpass XP_STEP   nonlinear part in real space          :1188-1209
@@ -29,15 +31,15 @@ namespace pfcg {
 template <typename T> struct FftCfg;
 template <> struct FftCfg<float> { static constexpr int MAXE = 16; };
 template <> struct FftCfg<double> { static constexpr int MAXE = 8; };
+// and of the runtime-plan kernels, in both precisions: 16 elements per thread
+// let 512 threads hold one 8192-point sequence (and 7168 / 7680 with a factor 7 / 5)
+constexpr int RT_MAXE = 16;
 // Main radix (elements per thread) of the kernels specialised on the length N:
 // FftCfg's, except FP32 384 = 8 * 6 * 8, which has no radix-16 form with
 // radix-16 first and last passes.
 template <typename T> __host__ __device__ constexpr int ct_maxe(int N) {
 	return (sizeof(T) == 4 && N == 384) ? 8 : FftCfg<T>::MAXE;
 }
-// and of the runtime-plan kernels, in both precisions: 16 elements per thread
-// let 512 threads hold one 8192-point sequence (and 7168 / 7680 with a factor 7 / 5)
-constexpr int RT_MAXE = 16;
 constexpr int MAXNT = 512; // threads per CTA of the FFT kernels
 
 
