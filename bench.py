@@ -140,9 +140,10 @@ def traffic_from_profiles(kernel: str, workload_name: str):
         return None
 
 
-def cpu_baseline(N: int, U: int, rank: int, steps: int):
+def cpu_baseline(N: int, U: int, rank: int, steps: int, warmup: int = 1):
     """The reference solver's step (demos/honey/pfc-relax.c over the project FFT
-    shim, all host threads) timed on a bounded sample of the same workload."""
+    shim, all host threads) timed on a bounded sample of the same workload:
+    `warmup` untimed steps, then `steps` timed ones."""
     exe = os.path.join(ROOT, "oracle", "_ref", "pfc-relax-bench")
     if not os.path.exists(exe):
         return None
@@ -157,16 +158,16 @@ def cpu_baseline(N: int, U: int, rank: int, steps: int):
         env = dict(os.environ)
         threads = os.cpu_count() or 1
         env["OMP_NUM_THREADS"] = str(threads)
-        r = subprocess.run([exe, "x.in", "fields.bin", "1", str(steps)], cwd=d, capture_output=True, text=True,
-                           env=env, timeout=900)
+        r = subprocess.run([exe, "x.in", "fields.bin", str(warmup), str(steps)], cwd=d, capture_output=True,
+                           text=True, env=env, timeout=900)
         if r.returncode != 0:
             return {"error": r.stderr[-300:]}
         res = json.loads(r.stdout.strip().splitlines()[-1])
     return {"value": res["steps"] / res["seconds"], "unit": "steps/s", "cores": res["threads"],
             "kind": "reference",
-            "sample": "%d steps of %dx%d U=%d after 1 warm-up step; reference step() over the project FFT shim "
+            "sample": "%d steps of %dx%d U=%d after %d warm-up steps; reference step() over the project FFT shim "
                       "(not FFTW), %d OpenMP threads in the FFT, pointwise loops single-threaded"
-                      % (res["steps"], N, N, U, res["threads"])}
+                      % (res["steps"], N, N, U, warmup, res["threads"])}
 
 
 def batch_problems(seed: int = 7, n: int = 96):
@@ -194,48 +195,64 @@ def batch_problems(seed: int = 7, n: int = 96):
     return out
 
 
-def run_batch(args):
+def batch_record(steps: int, warmup: int) -> dict:
     """Config C4: aggregate grid-point updates/s of the batched launch (two
     kernels per step for each class of problems of one size and field count,
     the classes side by side, steps captured in one CUDA graph) against the
-    same problems relaxed one after another through their own handles."""
+    same problems relaxed one after another through their own handles. Both
+    timed with CUDA events on their streams around `steps` steps after
+    `warmup` untimed ones."""
     import torch
 
     probs = batch_problems()
     upd = sum(p[0].U * p[1] * p[2] for p in probs)
-    K = args.steps
     res = {}
     with lib.Batch([p[:5] for p in probs], "fp32", autotune=True) as b:
         for prob, p in zip(b.problems, probs):
             prob.upload(p[5])
-        b.step(args.warmup)
+        b.step(warmup)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        b.step(K)
-        dt = time.perf_counter() - t0
-        res["batched"] = {"updates_per_s": upd * K / dt, "ms_per_step": dt / K * 1e3,
-                          "kernel_launches_per_step": b.launches(1)[0],
-                          "graph_launches": 1}
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.ExternalStream(b.stream)
+        e0.record(st)
+        b.step(steps)
+        e1.record(st)
+        torch.cuda.synchronize()
+        dt = e0.elapsed_time(e1) * 1e-3
+        res["batched"] = {"updates_per_s": upd * steps / dt, "ms_per_step": dt / steps * 1e3,
+                          "kernel_launches_per_step": b.launches(1)[0], "graph_launches_per_call": 1}
         rs = [lib.Relaxation(*p[:5], "fp32") for p in probs]
     for r, p in zip(rs, probs):
         r.autotune(5)
         r.upload(p[5])
-        r.step(args.warmup)
+        r.step(warmup)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for r in rs:
-        r.step(K)
+        r.step(steps)
+    torch.cuda.synchronize()
     dt = time.perf_counter() - t0
-    res["sequential"] = {"updates_per_s": upd * K / dt, "ms_per_step": dt / K * 1e3,
-                         "kernel_launches_per_step": 2 * len(probs)}
+    res["sequential"] = {"updates_per_s": upd * steps / dt, "ms_per_step": dt / steps * 1e3,
+                         "kernel_launches_per_step": 2 * len(probs),
+                         "timing": "wall clock around the 96 handles' calls, one after another"}
     for r in rs:
         r.close()
+    res.update(problems=len(probs), points_x_fields_per_step=upd, steps=steps, warmup=warmup,
+               speedup_vs_sequential=res["batched"]["updates_per_s"] / res["sequential"]["updates_per_s"],
+               unit="grid-point updates/s")
+    return res
+
+
+def run_batch(args):
+    """--batch: the C4 line on its own."""
+    res = batch_record(args.steps, args.warmup)
     line = {"metric": "batched relaxation, aggregate grid-point updates/s (96 problems, sizes 256-1536, U 1-2)",
             "value": res["batched"]["updates_per_s"], "unit": "grid-point updates/s", "higher_is_better": True,
-            "steps": K, "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batch96_mixed", "problems": len(probs), "points_x_fields_per_step": upd},
+            "steps": args.steps, "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch96_mixed", "problems": res["problems"],
+                       "points_x_fields_per_step": res["points_x_fields_per_step"]},
             "batched": res["batched"], "sequential": res["sequential"],
-            "speedup_vs_sequential": res["batched"]["updates_per_s"] / res["sequential"]["updates_per_s"]}
+            "speedup_vs_sequential": res["speedup_vs_sequential"]}
     print(json.dumps(line))
 
 
@@ -244,10 +261,13 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     N, U = args.size, 2
-    steps = max(2, min(args.steps, args.cpu_steps))
+    # the same step and warm-up counts as the GPU arm, bounded so that the run
+    # stays within about a minute of host time at 4096^2
+    steps = max(1, min(args.steps, args.ref_max_steps))
+    warm = max(1, min(args.warmup, 10))
     per = []
     for _ in range(max(1, args.reps)):
-        cb = cpu_baseline(N, U, rank, steps)
+        cb = cpu_baseline(N, U, rank, steps, warm)
         if cb is None or "error" in cb:
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pfc-relax-bench missing or failed: %s"
                               % (cb or {}).get("error", "not built")}))
@@ -256,9 +276,11 @@ def run_reference(args, rank, world):
     v = statistics.median(c["value"] for c in per)
     cb = per[0]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
-            "steps": steps, "warmup": 1, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "steps": steps, "warmup": warm, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "hetero2c_%dx%d" % (N, N), "U": U, "grid": [N, N], "l2": "inputs larger than L2"},
+            "config": {"workload": "hetero2c_%dx%d" % (N, N), "U": U, "grid": [N, N], "dt": 0.25, "dynamics": "conserved",
+                       "precision": "fp64 (the reference's only precision)", "parallelism": "one process",
+                       "l2": "inputs larger than L2"},
             "cpu_baseline": {"value": v, "unit": "steps/s", "cores": cb["cores"], "kind": "reference",
                              "sample": cb["sample"]},
             "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -285,38 +307,61 @@ def accuracy_profile(params, N, dx, dy, f0, marks=(10, 100, 300)):
 
 def run_ttr(args):
     """Time to relaxed on the 4096^2 two-field workload: steps until the mean
-    free energy changes by less than 1e-9 per step over a 100-step window,
-    with the wall time of the whole run (every step and evaluation, and for the
-    warm start the network's tiled application). Three arms from the same
-    initial state: the plain FP64 iteration (the reference precision), the plain FP32
-    iteration, and FP32 with the learned warm start (the network's input step of
-    plain steps, the network, then the plain finish). Creating the network and
-    loading its weights is reported apart, as set-up."""
+    free energy changes by less than 1e-9 per step over a 100-step window, with
+    the box optimised every 100 steps (the heterostructure configuration's box
+    optimisation), and the wall time of the whole run (every step, evaluation
+    and optimisation, and for the warm start the network's tiled application).
+    Arms from the same initial state: the plain FP64 iteration (the reference
+    precision), the same from the initial state moved by one ulp (the control:
+    how far two FP64 runs end apart), the plain FP32 iteration, and FP32 with the
+    learned warm start (the network's input step of plain steps, the network,
+    then the plain finish). Creating the network and loading its weights is
+    reported apart, as set-up."""
     lib.set_device(0)
-    arms = ttr_arms(args.size, args.ttr_max_steps)
     N = args.size
+    reps = []
+    for _ in range(max(1, args.ttr_reps)):
+        reps.append(ttr_arms(N, args.ttr_max_steps, args.ttr_topt))
+    arms = ttr_median(reps)
     line = {"metric": "time to relaxed (|d<f>|/step < 1e-9), %dx%d two-field heterostructure" % (N, N),
             "value": arms["warm_fp32"]["seconds"], "unit": "s", "higher_is_better": False,
             "dtype": "f32", "data": "synthetic", "n_gpus": 1,
             "config": {"workload": "hetero2c_%dx%d" % (N, N), "criterion": "|<f>(t) - <f>(t-100)| / 100 < 1e-9",
-                       "evaluate_every": 100},
-            "arms": arms}
+                       "evaluate_every": 100, "box_optimisation_every": args.ttr_topt, "repeats": len(reps)},
+            "arms": arms, "repeats": reps if len(reps) > 1 else None}
     print(json.dumps(line))
 
 
-def ttr_arms(N: int, max_steps: int) -> dict:
-    """The three time-to-relaxed arms (see run_ttr) on the N x N workload."""
+def ttr_median(reps):
+    """Per arm, the repeat with the median time (all fields of that repeat)."""
+    if len(reps) == 1:
+        return reps[0]
+    out = {}
+    for name in reps[0]:
+        runs = sorted((r[name] for r in reps), key=lambda a: a["seconds"])
+        out[name] = dict(runs[len(runs) // 2], seconds_all=[a["seconds"] for a in runs])
+    return out
+
+
+TTR_TOL = 1e-9
+TTR_EVERY = 100
+
+
+def ttr_arms(N: int, max_steps: int, Topt: int = 100) -> dict:
+    """The time-to-relaxed arms (see run_ttr) on the N x N workload."""
     import torch
 
     from pfc_b200 import fno
 
     pd, dx, dy, f0 = workload(N, 0)
     params = P.make_params(pd, 1.0, 0.25)
+    # the control: every initial value moved up by one unit in the last place
+    f0_ulp = np.nextafter(f0, np.inf)
     arms = {}
-    for name, prec, warm in (("plain_fp64", "fp64", False), ("plain_fp32", "fp32", False),
-                             ("warm_fp32", "fp32", True)):
+    for name, prec, warm, state in (("plain_fp64", "fp64", False, f0), ("control_fp64_1ulp", "fp64", False, f0_ulp),
+                                    ("plain_fp32", "fp32", False, f0), ("warm_fp32", "fp32", True, f0)):
         r = lib.Relaxation(params, N, N, dx, dy, prec)
-        r.upload(f0)
+        r.upload(state)
         rec = {}
         net = None
         if warm:
@@ -331,18 +376,22 @@ def ttr_arms(N: int, max_steps: int) -> dict:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         pre = 0
+        d = 1e-4
         if warm:
             # the network's input is the state after its input step of plain FP32 steps
             pre = int(meta.get("input_step", 0))
-            r.step(pre)
+            for t in range(0, pre, TTR_EVERY):
+                r.step(TTR_EVERY)
+                if Topt > 0 and (t + TTR_EVERY) % Topt == 0:
+                    d = r.optimize(1, 1, d)
             t1 = time.perf_counter()
             r.warmstart(net)
             torch.cuda.synchronize()
             rec["network_s"] = time.perf_counter() - t1
             rec["f_after_network"] = r.evaluate()[0]
-        steps, fave, _ = r.relax_until(1e-9, 100, max_steps)
+        steps, fave, _ = r.relax_until(TTR_TOL, TTR_EVERY, max_steps, Topt=Topt, d=d)
         rec.update(seconds=time.perf_counter() - t0, steps=None if steps is None else steps + pre, fave=fave,
-                   relaxed=steps is not None, plain_steps_before_network=pre)
+                   relaxed=steps is not None, plain_steps_before_network=pre, box=list(r.box()))
         arms[name] = rec
         r.close()
         if net:
@@ -350,6 +399,7 @@ def ttr_arms(N: int, max_steps: int) -> dict:
     f64 = arms["plain_fp64"]
     for rec in arms.values():
         rec["rel_dF_vs_plain_fp64"] = abs(rec["fave"] - f64["fave"]) / abs(f64["fave"])
+        rec["rel_dbox_vs_plain_fp64"] = max(abs(a - b) / b for a, b in zip(rec["box"], f64["box"]))
         rec["speedup_vs_plain_fp64"] = f64["seconds"] / rec["seconds"]
     return arms
 
@@ -362,14 +412,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--size", type=int, default=4096)
-    ap.add_argument("--cpu-steps", type=int, default=6, help="reference steps in the CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=6, help="reference steps in the CPU sample of the GPU arm")
+    ap.add_argument("--ref-max-steps", type=int, default=60, help="cap on the steps of --impl reference")
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT reference timing")
     ap.add_argument("--batch", action="store_true", help="the batched workload (96 mixed problems) instead")
+    ap.add_argument("--no-batch", action="store_true", help="leave the batched workload out of the default line")
+    ap.add_argument("--batch-steps", type=int, default=200, help="timed steps of the batch record")
     ap.add_argument("--ttr", action="store_true", help="time to relaxed: plain FP64, plain FP32, warm-started FP32")
     ap.add_argument("--ttr-max-steps", type=int, default=80000)
+    ap.add_argument("--ttr-topt", type=int, default=100, help="box optimisation period of the time-to-relaxed arms")
+    ap.add_argument("--ttr-reps", type=int, default=1, help="repeats of the time-to-relaxed arms (median reported)")
     ap.add_argument("--no-ttr", action="store_true", help="leave the time-to-relaxed arms out of the default line")
     args = ap.parse_args()
 
@@ -512,7 +567,7 @@ def main():
         "metric": METRIC, "value": steps_per_s, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if main_p == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": wl_name, "U": U, "grid": [N, N], "dt": 0.25, "dynamics": "conserved",
+        "config": {"workload": "hetero2c_%dx%d" % (N, N), "U": U, "grid": [N, N], "dt": 0.25, "dynamics": "conserved",
                    "precision": main_p + " FFT/pointwise, fp64 reductions and k=0 mode",
                    "parallelism": "replicas x%d" % world, "l2": "inputs larger than L2 (268 MB working set)"},
         "gpu_launches": res["launches"],
@@ -532,12 +587,16 @@ def main():
                         "fave": r64["fave"], "rel_dF_vs_fp32": abs(res["fave"] - r64["fave"]) / abs(r64["fave"])}
     if acc:
         line["accuracy_fp32_vs_fp64"] = acc
+    if rank == 0 and world == 1 and not args.no_batch and main_p == "fp32":
+        line["batch"] = batch_record(args.batch_steps, max(3, args.warmup))
     if rank == 0 and world == 1 and not args.no_ttr and main_p == "fp32":
         for v in results.values():
             v["r"].close()
         results = {}
         line["time_to_relaxed"] = {"criterion": "|<f>(t) - <f>(t-100)| / 100 < 1e-9, <f> every 100 steps",
-                                   "unit": "s (wall, whole run)", "arms": ttr_arms(N, args.ttr_max_steps)}
+                                   "box_optimisation_every": args.ttr_topt,
+                                   "unit": "s (wall, whole run)",
+                                   "arms": ttr_arms(N, args.ttr_max_steps, args.ttr_topt)}
     if cpu:
         line["cpu_baseline"] = cpu
     if cufft:

@@ -125,10 +125,62 @@ typedef struct pfcg_hetero {
 int pfcg_init_hetero(double* d_fields, int Nx, int Ny, double dx, double dy, const pfcg_hetero* s, void* stream);
 const char* pfcg_init_last_error(void);
 
+/* One grain of the reference builder's Voronoi step "V" (src/PFCInit.java:389-462,
+ * fields in its input order): centre (x, y) (wrapped into the box), write type
+ * (0 overwrite, 1 superpose, 2 phantom: the point is left as it is), lattice
+ * symmetry (3 triangular, 4 square, 6 honeycomb), length scale a, average
+ * density nave, amplitude amp, noise amplitude namp, and the placement tx1,
+ * ty1, theta (degrees), rotation axis xr, yr, tx2, ty2. */
+typedef struct pfcg_grain {
+	double x, y;
+	int type, sym;
+	double a, nave, amp, namp;
+	double tx1, ty1, theta_deg, xr, yr, tx2, ty2;
+} pfcg_grain;
+
+/* The Voronoi step on one field (Ny*Nx doubles, y-major; DEVICE or HOST memory,
+ * told apart by cudaPointerGetAttributes), read and written in place: each point takes the grain whose centre is nearest under
+ * periodic boundaries (closest(), src/PFCInit.java:68-93) and becomes
+ * type * old + nave + amp * OMA(r') + 2 namp (U - 0.5) (:444-458), OMA the
+ * one-mode lattice of :46-66. U is java.util.Random's nextDouble, drawn once
+ * per non-phantom point in row-major order as the Java loop does; *rng is the
+ * generator's 48-bit state (pfcg_java_random_seed(seed) for new Random(seed)),
+ * advanced past the draws on return, so consecutive steps continue one
+ * sequence. Allocates and frees its own scratch; synchronises `stream`. */
+int pfcg_init_voronoi(double* field, int Nx, int Ny, double dx, double dy, int ngrains, const pfcg_grain* grains,
+                      long long* rng, void* stream);
+
+/* The 48-bit state of java.util.Random(seed) (its documented initial scramble). */
+long long pfcg_java_random_seed(long long seed);
+
+/* Writes a density field as the reference builder's output step "O" does
+ * (src/PFCInit.java:670-686): "Nx Ny " then dx and dy in Java's "%.{prec}e",
+ * then the Nx*Ny values (y-major) one per line in the same format. Java's
+ * Formatter rounds the shortest round-trip decimal digits half-up where C's
+ * printf rounds the exact binary value (ties to even), so the two differ on
+ * values whose shortest digits end in a 5 just past the last printed digit;
+ * this writer follows Java (exactly for prec <= 13). HOST memory; returns 0, or
+ * PFCG_EARG when the file cannot be written. */
+int pfcg_write_n_pfcinit(const char* path, int Nx, int Ny, double dx, double dy, const double* field, int prec);
+
 /* Sets the grid spacing and rebuilds the linear operators. Replaces update_AB
  * (:901-958) after a change of s->dx, s->dy. */
 int pfcg_set_box(pfcg_handle* h, double dx, double dy);
 int pfcg_get_box(const pfcg_handle* h, double* dx, double* dy);
+
+/* Time integration scheme of pfcg_step (and of a batch's steps, which pick up
+ * the change at their next pfcg_batch_step). PFCG_SCHEME_ETD1, the default, is
+ * the reference's exponential update N' = A N + B M with A = exp(o a dt),
+ * B = (A - 1)/a (update_AB, pfc-relax.c:947-953, applied in step :1238).
+ * PFCG_SCHEME_SEMI_IMPLICIT treats the linear part implicitly and the rest
+ * explicitly: N' = (N + dt o M) / (1 - dt o a), i.e. for conserved dynamics
+ * (o = -k^2) N' = (N - dt k^2 M) / (1 + dt k^2 a(k)); it has the same fixed
+ * points but no counterpart in the reference. Returns PFCG_EARG for an unknown
+ * scheme. */
+#define PFCG_SCHEME_ETD1 0
+#define PFCG_SCHEME_SEMI_IMPLICIT 1
+int pfcg_set_scheme(pfcg_handle* h, int scheme);
+int pfcg_get_scheme(const pfcg_handle* h, int* scheme);
 
 /* Relaxation step counter t used for the every-100-steps resynchronisation of
  * the spectral state (:1179-1185). pfcg_upload sets t = 0, pfcg_step advances it. */
@@ -215,6 +267,7 @@ int pfcg_batch_create(int nprob, const pfcg_params* params, const int* Nx, const
 pfcg_handle* pfcg_batch_problem(pfcg_batch* b, int i);
 int pfcg_batch_step(pfcg_batch* b, int nsteps); /* 39 if any problem saw a NaN */
 int pfcg_batch_launches(const pfcg_batch* b, int nsteps, long long* kernels, long long* graph_launches);
+int pfcg_batch_stream(const pfcg_batch* b, void** stream); /* the cudaStream_t the batch launches on, for timing */
 void pfcg_batch_destroy(pfcg_batch* b);
 
 /* ---- Learned warm start. No counterpart in the reference. ----
@@ -274,14 +327,19 @@ void pfcg_fno_destroy(pfcg_fno* f);
  *   allocates it; the call itself allocates nothing.
  * stream: a cudaStream_t (NULL = the default stream); the call returns after it
  *   has synchronised with that stream.
- * Transforms run in FP32 (means and reductions in FP64), as PFCG_FP32.
+ * Transforms run in FP32 (means and reductions in FP64), as PFCG_FP32, on the
+ * runtime-plan step kernels only: the kernels specialised on a length need
+ * per-pass twiddle tables that this call does not build, so at those lengths a
+ * step costs more than through a handle (512^2 U=1: about 59 us against 24 us
+ * on a B200).
  * The workspace is a file-scope array of PFCG_NOALLOC_SCRATCH_BYTES (32 MiB)
  * that every GPU loading the library holds until exit; grids needing more,
  * about 2 * U * (Nx/2+1) * Ny * 8 bytes plus a few KB, are rejected with
- * PFCG_ESIZE. The first call on a device takes the array's device address
- * (cudaGetSymbolAddress) and sets kernel attributes; make that first call
- * before any stream capture. All calls share the one array and it keeps the
- * last call's contents (the call clears what must start at zero), so calls
+ * PFCG_ESIZE. Every call looks up the array's address on the current device
+ * (cudaGetSymbolAddress, which allocates nothing). The first call on a device
+ * also sets kernel attributes (cudaFuncSetAttribute); make that first call
+ * before any stream capture begins. All calls share the one array and it keeps
+ * the last call's contents (the call clears what must start at zero), so calls
  * that overlap on the GPU (other streams, other host threads) race.
  * Returns 0, 39 on NaN, or a negative PFCG_E* code (pfcg_last_error(NULL)). */
 int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double dx, double dy, int nsteps, double* fields,

@@ -43,6 +43,7 @@ typedef struct pfco {
 	double dx, dy;
 	int t;
 	int emulate_nu2;
+	int scheme;                /* 0 ETD1 (the reference), 1 semi-implicit (pfco_set_scheme) */
 	double* m[PFCG_MAX_U];     /* real fields, Ny x Nx */
 	fft64_cplx* N[PFCG_MAX_U]; /* spectral state / (Nx Ny), H x Ny transposed */
 	fft64_cplx* M[PFCG_MAX_U]; /* work spectra */
@@ -85,6 +86,13 @@ static void update_AB(pfco* o) {
 			for (int u = 0; u < o->U; u++) {
 				const double a = p->alpha[u][u] + p->beta[u][u] * P_of(p, u, k2);
 				const double om = c - 1.0 - c * k2;
+				if (o->scheme == 1) {
+					/* semi-implicit: (N + dt o M) / (1 - dt o a), no counterpart in the reference */
+					const double den = 1.0 - om * a * p->dt;
+					o->A[u][ij] = 1.0 / den;
+					o->B[u][ij] = om * p->dt / den * inv;
+					continue;
+				}
 				const double ex = exp(om * a * p->dt);
 				o->A[u][ij] = ex;
 				o->B[u][ij] = ((a == 0.0) ? om * p->dt : (ex - 1.0) / a) * inv;
@@ -133,6 +141,14 @@ void pfco_destroy(pfco* o) {
 }
 
 void pfco_set_emulate_nu2(pfco* o, int on) { o->emulate_nu2 = on; }
+
+/* Time integrator: 0 = ETD1 (update_AB, :947-953), 1 = the semi-implicit update
+ * N' = (N + dt o M) / (1 - dt o a) (o = c - 1 - c k^2), which the reference does
+ * not have; the restatement of the formula lives in update_AB above. */
+void pfco_set_scheme(pfco* o, int scheme) {
+	o->scheme = scheme;
+	update_AB(o);
+}
 
 void pfco_upload(pfco* o, const double* fields) {
 	for (int u = 0; u < o->U; u++) memcpy(o->m[u], fields + (size_t)u * npts(o), npts(o) * sizeof(double));

@@ -41,6 +41,7 @@ def lib():
         L.pfco_evaluate.argtypes = [vp, dp, dp, dp]
         L.pfco_optimize.argtypes = [vp, ip, ip, dp]
         L.pfco_set_emulate_nu2.argtypes = [vp, ip]
+        L.pfco_set_scheme.argtypes = [vp, ip]
         L.fft64_r2c_2d_tr.argtypes = [ip, ip, dp, ctypes.c_ssize_t, dp]
         L.fft64_c2r_2d_tr.argtypes = [ip, ip, dp, dp, ctypes.c_ssize_t]
         L.fft64_prepare_2d.argtypes = [ip, ip]
@@ -143,6 +144,10 @@ class Oracle:
 
     def emulate_nu2(self, on=True):
         self.L.pfco_set_emulate_nu2(self.h, 1 if on else 0)
+
+    def set_scheme(self, scheme: str):
+        """'etd1' (the reference) or 'semi' (the semi-implicit update, not in the reference)."""
+        self.L.pfco_set_scheme(self.h, {"etd1": 0, "semi": 1}[scheme])
 
     def relax(self, tend: int, Tprint: int, Topt: int = 0, xopt: int = 1, yopt: int = 1):
         """The reference's relax() schedule (pfc-relax.c:1293-1313) without file

@@ -1024,6 +1024,20 @@ int pfcg_set_box(pfcg_handle* h, double dx, double dy) {
 	return 0;
 }
 
+int pfcg_set_scheme(pfcg_handle* h, int scheme) {
+	if (!h) return PFCG_EARG;
+	if (scheme != PFCG_SCHEME_ETD1 && scheme != PFCG_SCHEME_SEMI_IMPLICIT)
+		return fail(h, PFCG_EARG, "unknown time integration scheme");
+	h->model.scheme = scheme == PFCG_SCHEME_SEMI_IMPLICIT ? SCHEME_SEMI : SCHEME_ETD1;
+	return 0;
+}
+
+int pfcg_get_scheme(const pfcg_handle* h, int* scheme) {
+	if (!h || !scheme) return PFCG_EARG;
+	*scheme = h->model.scheme == SCHEME_SEMI ? PFCG_SCHEME_SEMI_IMPLICIT : PFCG_SCHEME_ETD1;
+	return 0;
+}
+
 int pfcg_get_box(const pfcg_handle* h, double* dx, double* dy) {
 	if (!h || !dx || !dy) return PFCG_EARG;
 	*dx = h->geom.dx;
@@ -1197,6 +1211,7 @@ struct pfcg_batch {
 	int xblocks = 0, yblocks = 0;
 	std::vector<BatchClass> cls;
 	std::map<int, cudaGraphExec_t> graphs;
+	std::vector<unsigned char> hargs; // host copy of the x and y argument arrays last uploaded
 	std::string err;
 };
 
@@ -1205,14 +1220,11 @@ static bool batch_ct(const pfcg_handle* h) { return h->cxs.spec && h->cys.spec &
 
 namespace {
 
-template <typename T> int batch_build(pfcg_batch* b) {
+// per-problem kernel arguments of a batch from the problems' handles
+template <typename T> void batch_args(pfcg_batch* b, std::vector<XArgs<T>>& xa, std::vector<YArgs<T>>& ya) {
 	const int n = (int)b->h.size();
-	auto bfail = [&](cudaError_t e, const char* what) {
-		b->err = std::string(what) + ": " + cudaGetErrorString(e);
-		return PFCG_ECUDA;
-	};
-	std::vector<XArgs<T>> xa(n);
-	std::vector<YArgs<T>> ya(n);
+	xa.assign(n, XArgs<T>{});
+	ya.assign(n, YArgs<T>{});
 	for (int i = 0; i < n; i++) {
 		pfcg_handle* h = b->h[i];
 		xa[i] = xargs<T>(h);
@@ -1220,6 +1232,40 @@ template <typename T> int batch_build(pfcg_batch* b) {
 		xa[i].flag = b->d_flags + i;
 		ya[i] = yargs<T>(h);
 	}
+}
+
+// Re-uploads the argument arrays the step graphs read when a problem's box or
+// scheme changed since the last upload (pfcg_optimize / pfcg_set_box /
+// pfcg_set_scheme on a problem handle), ordered on the batch stream.
+template <typename T> int batch_refresh_args(pfcg_batch* b) {
+	std::vector<XArgs<T>> xa;
+	std::vector<YArgs<T>> ya;
+	batch_args<T>(b, xa, ya);
+	const size_t bx = sizeof(XArgs<T>) * xa.size(), by = sizeof(YArgs<T>) * ya.size();
+	std::vector<unsigned char> cur(bx + by);
+	memcpy(cur.data(), xa.data(), bx);
+	memcpy(cur.data() + bx, ya.data(), by);
+	if (cur == b->hargs) return 0;
+	cudaError_t e = cudaMemcpyAsync(b->d_xargs, xa.data(), bx, cudaMemcpyHostToDevice, b->stream);
+	if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_yargs, ya.data(), by, cudaMemcpyHostToDevice, b->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+	if (e != cudaSuccess) {
+		b->err = std::string("batch arguments: ") + cudaGetErrorString(e);
+		return PFCG_ECUDA;
+	}
+	b->hargs.swap(cur);
+	return 0;
+}
+
+template <typename T> int batch_build(pfcg_batch* b) {
+	const int n = (int)b->h.size();
+	auto bfail = [&](cudaError_t e, const char* what) {
+		b->err = std::string(what) + ": " + cudaGetErrorString(e);
+		return PFCG_ECUDA;
+	};
+	std::vector<XArgs<T>> xa;
+	std::vector<YArgs<T>> ya;
+	batch_args<T>(b, xa, ya);
 	// classes: one per (U, N) with specialised kernels, one for the rest
 	std::map<std::pair<int, int>, int> key;
 	std::vector<std::vector<int>> members;
@@ -1291,6 +1337,9 @@ template <typename T> int batch_build(pfcg_batch* b) {
 	if ((e = cudaMalloc(&b->d_blk, sizeof(int) * (2 * xp.size() + 2 * yp.size()))) != cudaSuccess) return bfail(e, "cudaMalloc");
 	cudaMemcpy(b->d_xargs, xa.data(), sizeof(XArgs<T>) * n, cudaMemcpyHostToDevice);
 	cudaMemcpy(b->d_yargs, ya.data(), sizeof(YArgs<T>) * n, cudaMemcpyHostToDevice);
+	b->hargs.resize(sizeof(XArgs<T>) * n + sizeof(YArgs<T>) * n);
+	memcpy(b->hargs.data(), xa.data(), sizeof(XArgs<T>) * n);
+	memcpy(b->hargs.data() + sizeof(XArgs<T>) * n, ya.data(), sizeof(YArgs<T>) * n);
 	int* q = b->d_blk;
 	cudaMemcpy(q, xp.data(), sizeof(int) * xp.size(), cudaMemcpyHostToDevice);
 	cudaMemcpy(q + xp.size(), xl.data(), sizeof(int) * xl.size(), cudaMemcpyHostToDevice);
@@ -1405,6 +1454,8 @@ int pfcg_batch_step(pfcg_batch* b, int nsteps) {
 		if (e != cudaSuccess) { b->err = cudaGetErrorString(e); g_err = b->err; return PFCG_ECUDA; }
 		it = b->graphs.emplace(nsteps, ge).first;
 	}
+	const int ra = b->prec == PFCG_FP64 ? batch_refresh_args<double>(b) : batch_refresh_args<float>(b);
+	if (ra) { g_err = b->err; return ra; }
 	cudaError_t e = cudaGraphLaunch(it->second, b->stream);
 	const int n = (int)b->h.size();
 	if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_flags, b->d_flags, sizeof(int) * n, cudaMemcpyDeviceToHost, b->stream);
@@ -1416,6 +1467,12 @@ int pfcg_batch_step(pfcg_batch* b, int nsteps) {
 	}
 	for (int i = 0; i < n; i++)
 		if (b->h_flags[i]) { g_err = "Not a number value detected."; return PFCG_NAN; }
+	return 0;
+}
+
+int pfcg_batch_stream(const pfcg_batch* b, void** stream) {
+	if (!b || !stream) return PFCG_EARG;
+	*stream = (void*)b->stream;
 	return 0;
 }
 
@@ -1452,14 +1509,13 @@ void pfcg_batch_destroy(pfcg_batch* b) {
 // device workspace lives in the file-scope array below instead of cudaMalloc'd
 // memory. Every GPU that loads this library holds the array until the process
 // exits. In host code g_noalloc_scratch names a host-side stand-in, not device
-// memory: its device address comes from cudaGetSymbolAddress, taken once per
-// device (with that device current) by the first call on it.
+// memory: every call looks up its device address on the current device with
+// cudaGetSymbolAddress (a host-side query that allocates nothing), so no
+// address is cached across calls, contexts or host threads.
 
 namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PFCG_NOALLOC_SCRATCH_BYTES];
-
-void* g_noalloc_addr[64];
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -1501,18 +1557,15 @@ extern "C" int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double d
 	int dev = 0;
 	cudaError_t e = cudaGetDevice(&dev);
 	if (e != cudaSuccess) return fail(nullptr, PFCG_ENODEV, cudaGetErrorString(e));
-	if (dev < 0 || dev >= 64) return fail(nullptr, PFCG_ENODEV, "device index out of range");
 	cudaDeviceProp prop;
 	e = cudaGetDeviceProperties(&prop, dev);
 	if (e != cudaSuccess) return fail(nullptr, PFCG_ENODEV, cudaGetErrorString(e));
 	if (prop.major != 10) return fail(nullptr, PFCG_ENODEV, "libpfc_b200 is built for sm_100a (B200) only");
-	if (!g_noalloc_addr[dev]) {
-		void* addr = nullptr;
-		e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
-		if (e != cudaSuccess || !addr)
-			return fail(nullptr, PFCG_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-		g_noalloc_addr[dev] = addr;
-	}
+	// the array's address on the current device, looked up on every call
+	void* scratch = nullptr;
+	e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+	if (e != cudaSuccess || !scratch)
+		return fail(nullptr, PFCG_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
 
 	// host-side description of the relaxation; no device memory is allocated
 	pfcg_handle h;
@@ -1540,7 +1593,7 @@ extern "C" int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double d
 	h.cxs = h.cx;
 	h.cys = h.cy;
 
-	unsigned char* base = (unsigned char*)g_noalloc_addr[dev];
+	unsigned char* base = (unsigned char*)scratch;
 	const size_t nspec = (size_t)h.H * Ny;
 	size_t off = 0;
 	auto carve = [&](size_t bytes) {

@@ -42,7 +42,16 @@ struct Model {
 	double lambda[MAXU], delta[MAXU];
 	double alpha[MAXU][MAXU], beta[MAXU][MAXU], gamma[MAXU][MAXU], epsilon[MAXU][MAXU], mu2[MAXU][MAXU];
 	double nu2[MAXU][MAXW], omega[MAXU][MAXW], phi[MAXU][MAXW];
+	int scheme; // SCHEME_ETD1 (the reference's update) or SCHEME_SEMI (linear part implicit)
 };
+
+// Time integrators of the k-space update N' = A N + B M (M the nonlinear and
+// coupling terms, x = o a dt with o = c - 1 - c k^2 and a the linear operator):
+//   SCHEME_ETD1  A = exp(x), B = (A - 1) / a, the reference's (pfc-relax.c:946-953)
+//   SCHEME_SEMI  A = 1 / (1 - x), B = o dt / (1 - x): the linear part implicit,
+//                the rest explicit, i.e. N' = (N - dt k^2 M) / (1 + dt k^2 a) for
+//                conserved dynamics. Same fixed points as ETD1.
+enum Scheme { SCHEME_ETD1 = 0, SCHEME_SEMI = 1 };
 
 struct Geom {
 	int Nx, Ny, H;

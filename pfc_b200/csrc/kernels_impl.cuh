@@ -147,6 +147,7 @@ template <typename T, int U, int NC, int CCC, int RC, bool FUSEDK = true> struct
 // precision (converting inside the per-entry loop costs an F2F per use).
 template <typename T, int U> struct StepConsts {
 	T invN, cc, dt, ag;
+	bool semi; // SCHEME_SEMI
 	int W[U];
 	T alpha[U], betad[U];
 	T nu2[U][MAXW], omega[U][MAXW], phi[U][MAXW];
@@ -156,6 +157,7 @@ template <typename T, int U> struct StepConsts {
 		cc = (T)m.c;
 		dt = (T)m.dt;
 		ag = (T)(-0.5 / m.sigma / m.sigma);
+		semi = m.scheme == SCHEME_SEMI;
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			W[u] = m.W[u];
@@ -210,6 +212,11 @@ __device__ __forceinline__ void entry_coef(const StepConsts<T, U>& K, T k2, T (&
 			}
 		const T av = K.alpha[u] + K.betad[u] * P;
 		const T x = o * av * K.dt;
+		if (K.semi) {
+			A[u] = (T)1 / ((T)1 - x);
+			Bn[u] = o * K.dt * A[u];
+			continue;
+		}
 		A[u] = expT<T>(x);
 		if constexpr (sizeof(T) == 4) Bn[u] = o * K.dt * phi1f(x, A[u]);
 		else Bn[u] = (av == (T)0) ? o * K.dt : etd_b<T>(A[u], x, av);
@@ -290,8 +297,14 @@ template <typename T, int U> __device__ __forceinline__ void ypass_mean_update(c
 		const double P0 = P_of<double>(a.m, u, 0.0);
 		const double av = a.m.alpha[u][u] + a.m.beta[u][u] * P0;
 		const double o = a.m.c - 1.0;
-		const double A = exp(o * av * a.m.dt);
-		const double B = ((av == 0.0) ? o * a.m.dt : (A - 1.0) / av) / NxNy;
+		double A, B;
+		if (a.m.scheme == SCHEME_SEMI) {
+			A = 1.0 / (1.0 - o * av * a.m.dt);
+			B = o * a.m.dt * A / NxNy;
+		} else {
+			A = exp(o * av * a.m.dt);
+			B = ((av == 0.0) ? o * a.m.dt : (A - 1.0) / av) / NxNy;
+		}
 		a.mean[u] = A * mean0[u] + B * Mk[u];
 		a.acc[u] = 0.0;
 	}
@@ -502,10 +515,15 @@ __device__ __forceinline__ void ypass_step_fused(const YArgs<T>& a, cplx<T>* sm,
 		const T av = alpha + betad * Pk;
 		const T o = K.cc - (T)1 - K.cc * k2;
 		const T x = o * av * K.dt;
-		const T A = expT<T>(x);
-		T Bn;
-		if constexpr (sizeof(T) == 4) Bn = o * K.dt * phi1f(x, A);
-		else Bn = (av == (T)0) ? o * K.dt : etd_b<T>(A, x, av);
+		T A, Bn;
+		if (K.semi) {
+			A = (T)1 / ((T)1 - x);
+			Bn = o * K.dt * A;
+		} else {
+			A = expT<T>(x);
+			if constexpr (sizeof(T) == 4) Bn = o * K.dt * phi1f(x, A);
+			else Bn = (av == (T)0) ? o * K.dt : etd_b<T>(A, x, av);
+		}
 		cplx<T> nn = cadd(cscale(Nown, A), cscale(M, Bn));
 		if (kx == 0 && ky == 0) nn = mk<T>((T)0, (T)0);
 		rb.v[0][r] = nn;
@@ -1383,6 +1401,14 @@ PFCG_CT_DECL(extern, 2, 1024)
 #if PFCG_CT_TU != 1536
 PFCG_CT_DECL(extern, 1, 1536)
 PFCG_CT_DECL(extern, 2, 1536)
+#endif
+#if PFCG_CT_TU != 2048
+PFCG_CT_DECL(extern, 1, 2048)
+PFCG_CT_DECL(extern, 2, 2048)
+#endif
+#if PFCG_CT_TU != 4096
+PFCG_CT_DECL(extern, 1, 4096)
+PFCG_CT_DECL(extern, 2, 4096)
 #endif
 
 template <typename T, int U> static cudaError_t ct_xdispatch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {

@@ -19,12 +19,24 @@ DRIVER_PATH = os.path.join(HERE, "pfc-relax")
 
 FP32, FP64 = 0, 1
 
+# time integration schemes of pfcg_set_scheme
+SCHEMES = {"etd1": 0, "semi": 1}
+
 OK = 0
 NAN = 39
 EARG, ECUDA, ESIZE, ENOMEM, ETIMEOUT, ENODEV = -1, -2, -3, -4, -5, -6
 
 # size of pfcg_relax_noalloc's static device workspace (PFCG_NOALLOC_SCRATCH_BYTES)
 NOALLOC_SCRATCH_BYTES = 32 << 20
+
+class Grain(ctypes.Structure):
+    """pfcg_grain: one grain of the builder's Voronoi step (include/pfc_b200.h)."""
+    _fields_ = [("x", ctypes.c_double), ("y", ctypes.c_double), ("type", ctypes.c_int), ("sym", ctypes.c_int),
+                ("a", ctypes.c_double), ("nave", ctypes.c_double), ("amp", ctypes.c_double),
+                ("namp", ctypes.c_double), ("tx1", ctypes.c_double), ("ty1", ctypes.c_double),
+                ("theta_deg", ctypes.c_double), ("xr", ctypes.c_double), ("yr", ctypes.c_double),
+                ("tx2", ctypes.c_double), ("ty2", ctypes.c_double)]
+
 
 # every entry point of include/pfc_b200.h with its ctypes signature
 _vp, _ip, _dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
@@ -39,8 +51,14 @@ SIGNATURES = {
     "pfcg_download_device": (ctypes.c_int, [_vp, _vp]),
     "pfcg_init_hetero": (ctypes.c_int, [_vp, _ip, _ip, ctypes.c_double, ctypes.c_double, _vp, _vp]),
     "pfcg_init_last_error": (ctypes.c_char_p, []),
+    "pfcg_init_voronoi": (ctypes.c_int, [_vp, _ip, _ip, ctypes.c_double, ctypes.c_double, _ip, _vp,
+                                         ctypes.POINTER(ctypes.c_longlong), _vp]),
+    "pfcg_java_random_seed": (ctypes.c_longlong, [ctypes.c_longlong]),
+    "pfcg_write_n_pfcinit": (ctypes.c_int, [ctypes.c_char_p, _ip, _ip, ctypes.c_double, ctypes.c_double, _dp, _ip]),
     "pfcg_set_box": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double]),
     "pfcg_get_box": (ctypes.c_int, [_vp, _dp, _dp]),
+    "pfcg_set_scheme": (ctypes.c_int, [_vp, _ip]),
+    "pfcg_get_scheme": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "pfcg_set_time": (ctypes.c_int, [_vp, _ip]),
     "pfcg_get_time": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "pfcg_step": (ctypes.c_int, [_vp, _ip]),
@@ -63,6 +81,7 @@ SIGNATURES = {
     "pfcg_batch_launches": (ctypes.c_int, [_vp, _ip, ctypes.POINTER(ctypes.c_longlong),
                                            ctypes.POINTER(ctypes.c_longlong)]),
     "pfcg_batch_destroy": (None, [_vp]),
+    "pfcg_batch_stream": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_void_p)]),
     "pfcg_fno_param_count": (ctypes.c_size_t, []),
     "pfcg_fno_create": (ctypes.c_int, [_ip, _ip, ctypes.POINTER(ctypes.c_void_p)]),
     "pfcg_fno_set_params": (ctypes.c_int, [_vp, _vp]),
@@ -130,7 +149,8 @@ class Relaxation:
     """One relaxation on the GPU: the state of pfc-relax's struct S for the hot
     path (fields, spectral state, box size, step counter)."""
 
-    def __init__(self, params: Params, Nx: int, Ny: int, dx: float, dy: float, precision: str = "fp64"):
+    def __init__(self, params: Params, Nx: int, Ny: int, dx: float, dy: float, precision: str = "fp64",
+                 scheme: str = "etd1"):
         self.L = load()
         self.params = params
         self.U = params.U
@@ -142,6 +162,18 @@ class Relaxation:
         if rc:
             raise PfcError(rc, self.L.pfcg_last_error(None).decode())
         self.h = h
+        if scheme != "etd1":
+            self.set_scheme(scheme)
+
+    def set_scheme(self, scheme: str) -> None:
+        """'etd1' (the reference's exponential update) or 'semi' (linear part implicit)."""
+        self._check(self.L.pfcg_set_scheme(self.h, SCHEMES[scheme]))
+
+    @property
+    def scheme(self) -> str:
+        v = ctypes.c_int()
+        self._check(self.L.pfcg_get_scheme(self.h, ctypes.byref(v)))
+        return {n: k for k, n in SCHEMES.items()}[v.value]
 
     def _check(self, rc: int):
         if rc:
@@ -283,18 +315,29 @@ class Relaxation:
             t = nxt
         return np.array(rows)
 
-    def relax_until(self, tol: float = 1e-9, every: int = 100, max_steps: int = 100000):
+    def relax_until(self, tol: float = 1e-9, every: int = 100, max_steps: int = 100000, Topt: int = 0,
+                    xopt: int = 1, yopt: int = 1, d: float = 1e-4, on_print=None):
         """Steps until the free energy changes by less than tol per step, measured
-        as |<f>(t) - <f>(t - every)| / every at every `every` steps. Returns
-        (steps taken, final <f>, seconds); steps is None if max_steps ran out."""
+        as |<f>(t) - <f>(t - every)| / every at every `every` steps. With Topt > 0
+        the box is optimised every Topt steps first, in the order of relax()
+        (pfc-relax.c:1297-1302: optimise, then evaluate, then step), starting
+        from the sampling step d; the criterion then compares <f> of the current
+        box. on_print(t, dx, dy, <f>) sees every evaluation. Returns (steps
+        taken, final <f>, seconds); steps is None if max_steps ran out."""
         import time
         t0 = time.perf_counter()
         prev = self.evaluate()[0]
+        if on_print:
+            on_print(0, *self.box(), prev)
         done = 0
         while done < max_steps:
             self.step(every)
             done += every
+            if Topt > 0 and done % Topt == 0:
+                d = self.optimize(xopt, yopt, d)
             f = self.evaluate()[0]
+            if on_print:
+                on_print(done, *self.box(), f)
             if abs(f - prev) / every < tol:
                 return done, f, time.perf_counter() - t0
             prev = f
@@ -393,6 +436,15 @@ class Batch:
         if rc:
             raise PfcError(rc, self.L.pfcg_last_error(None).decode())
         return rc
+
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t the batch launches on (for CUDA-event timing)."""
+        s = ctypes.c_void_p()
+        rc = self.L.pfcg_batch_stream(self.b, ctypes.byref(s))
+        if rc:
+            raise PfcError(rc, self.L.pfcg_last_error(None).decode())
+        return s.value or 0
 
     def launches(self, nsteps: int = 1):
         """(kernel launches, graph launches) of pfcg_batch_step(nsteps)."""

@@ -4,7 +4,11 @@
 - C2: 2048 x 2048 honeycomb polycrystal with box optimisation, 5000 steps, FP32
   against FP64.
 - C3: the 4096 x 4096 heterostructure, FP32 against FP64 over the first 100
-  steps of its (chaotic) transient, and exact conservation of both means.
+  steps of its (chaotic) transient, and exact conservation of both means; and
+  the configuration as specified, 10000 steps with the box optimised every 100
+  steps, FP32 against FP64 at every print (every 500 steps), with an FP64 run
+  from the initial state moved by one ulp as the control that measures how far
+  two FP64 runs drift apart over the same transient.
 
 Measured on B200 when these bounds were set:
 
@@ -87,3 +91,27 @@ def test_c3_heterostructure_4096_transient_and_means():
             out[prec] = r.evaluate()
             assert np.array_equal(out[prec][1], n_start)    # both means bit for bit
     assert abs(out["fp32"][0] - out["fp64"][0]) < 1e-6 * abs(out["fp64"][0])
+
+
+def test_c3_heterostructure_4096_box_optimisation_10000_steps():
+    pd = P.hetero_2c(0.04)
+    p = P.make_params(pd, 1.0, 0.25)
+    N, dx, a0 = 4096, 0.7, 7.2552
+    f0 = synth.stripes2(N, N, dx, dx, 512, (0.3, -0.3), (0.3, 0.3), (a0, a0 * 1.04), 0.02, 1000)
+    rows = {}
+    for name, prec, state in (("fp64", "fp64", f0), ("control", "fp64", np.nextafter(f0, np.inf)),
+                              ("fp32", "fp32", f0)):
+        with lib.Relaxation(p, N, N, dx, dx, prec) as r:
+            r.upload(state)
+            rows[name] = r.relax(10000, 500, 100)
+    a, c, b = rows["fp64"], rows["control"], rows["fp32"]
+    assert a.shape == b.shape == c.shape and a[-1, 0] == 10000
+    rel_f32 = np.abs(b[:, 3] - a[:, 3]) / np.abs(a[:, 3])
+    rel_ctl = np.abs(c[:, 3] - a[:, 3]) / np.abs(a[:, 3])
+    box_f32 = np.abs(b[:, 1:3] - a[:, 1:3]).max(axis=1) / a[:, 1]
+    box_ctl = np.abs(c[:, 1:3] - a[:, 1:3]).max(axis=1) / a[:, 1]
+    print("C3 box-opt: rel d<f> fp32", rel_f32.tolist(), "control", rel_ctl.tolist())
+    print("C3 box-opt: rel d(box) fp32", box_f32.tolist(), "control", box_ctl.tolist())
+    assert np.all(np.abs(b[:, 4:] - a[:, 4:]) < 1e-14)   # the means are conserved exactly
+    assert a[-1, 3] < a[0, 3] and a[-1, 1] != a[0, 1]     # relaxed, and the box did move
+    assert rel_f32.max() < 1e-4 and box_f32.max() < 1e-4

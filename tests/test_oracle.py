@@ -89,6 +89,30 @@ def test_linear_mode_grows_by_A():
     np.testing.assert_allclose(o.download()[0], f0 * A ** 3, atol=1e-15)
 
 
+def test_semi_implicit_linear_mode_known_answer():
+    """The oracle's semi-implicit variant (not in the reference): with gamma =
+    delta = lambda = 0 a single Fourier mode is multiplied by exactly
+    1 / (1 + dt k^2 a(k)) per step (conserved dynamics)."""
+    d = P.honeycomb_1c(-0.25)
+    d["delta"] = [0.0]
+    p = P.make_params(d, 1.0, 0.5)
+    Nx = Ny = 32
+    dx = dy = 0.9
+    o = pyoracle.Oracle(p, Nx, Ny, dx, dy)
+    o.set_scheme("semi")
+    x = np.arange(Nx) * dx
+    y = np.arange(Ny) * dy
+    kx = 2 * math.pi * 3 / (dx * Nx)
+    ky = 2 * math.pi * 2 / (dy * Ny)
+    f0 = 0.01 * np.cos(kx * x[None, :] + ky * y[:, None])
+    o.upload(f0[None])
+    o.step(3)
+    k2 = kx * kx + ky * ky
+    a = -0.25 + (1.0 - k2) ** 2
+    g = 1.0 / (1.0 + 0.5 * k2 * a)
+    np.testing.assert_allclose(o.download()[0], f0 * g ** 3, atol=1e-15)
+
+
 def test_optimize_moves_toward_unstrained_lattice():
     """A one-mode triangular lattice strained by 2% relaxes dx back toward the
     lattice's own spacing (pfc-relax.c:1251-1290)."""

@@ -6,11 +6,17 @@ device buffer of fields.
 
 Checked through the C ABI against the allocating entry points (pfcg_create,
 pfcg_upload, pfcg_step, pfcg_download) on two calls in a row, with different
-inputs, so a call that leaked state from the previous one would show. The test
-allocates its device buffer with torch; the entry point allocates nothing.
+inputs, so a call that leaked state from the previous one would show; against
+the FP64 CPU oracle at the FP32 parity bound of the other tests; and on a NaN
+input (return 39) followed by a clean call (return 0, so the NaN flag the
+first call left in the shared workspace was cleared). The test allocates its
+device buffers with torch; the entry point allocates nothing.
 This file is collected last so that a run stopping at the first failure has
 run every other test before it.
 """
+import os
+import sys
+
 import numpy as np
 import pytest
 
@@ -61,3 +67,46 @@ def test_noalloc_rejects_grids_beyond_its_workspace():
     rc = lib.relax_noalloc(p, Nx, Ny, 0.7, 0.7, 1, dev.data_ptr(), 0)
     assert rc == lib.ESIZE
     assert "static workspace" in lib.last_error()
+
+
+def test_noalloc_matches_oracle():
+    """The no-alloc relaxation against the FP64 CPU oracle (test infrastructure),
+    at the bounds the FP32 parity tests use: max |dpsi| < 2e-5, relative <f> 1e-6."""
+    import torch
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import pyoracle
+
+    Nx, Ny, dx, dy, nsteps = 96, 80, 0.7, 0.7, 60
+    p = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
+    f0 = synth.stripes2(Nx, Ny, dx, dy, 24, (0.3, -0.3), (0.3, 0.3), (7.2552, 7.2552 * 1.04), 0.02, 41)
+    o = pyoracle.Oracle(p, Nx, Ny, dx, dy)
+    o.upload(f0)
+    o.step(nsteps)
+    ref = o.download()
+    dev = torch.tensor(np.ascontiguousarray(f0), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(2):
+        dev.copy_(torch.tensor(np.ascontiguousarray(f0), dtype=torch.float64))
+        rc = lib.relax_noalloc(p, Nx, Ny, dx, dy, nsteps, dev.data_ptr(), 0)
+        assert rc == 0, lib.last_error()
+        got = dev.cpu().numpy().reshape(ref.shape)
+        assert np.abs(got - ref).max() < 2e-5, np.abs(got - ref).max()
+
+
+def test_noalloc_nan_then_clean_call():
+    """A NaN in the input returns the reference's code 39; the next clean call
+    returns 0, so the flag left in the shared workspace was cleared."""
+    import torch
+
+    Nx = Ny = 64
+    p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+    bad = synth.noise_state(Nx, Ny, 0.25, 0.05, 51)[None].copy()
+    bad[0, 3, 5] = np.nan
+    dev = torch.tensor(bad, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    assert lib.relax_noalloc(p, Nx, Ny, 0.7, 0.7, 5, dev.data_ptr(), 0) == lib.NAN
+    good = synth.noise_state(Nx, Ny, 0.25, 0.05, 52)[None]
+    dev = torch.tensor(np.ascontiguousarray(good), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    assert lib.relax_noalloc(p, Nx, Ny, 0.7, 0.7, 5, dev.data_ptr(), 0) == 0, lib.last_error()
