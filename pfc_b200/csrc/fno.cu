@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -98,84 +99,162 @@ __global__ void lift_fwd(const float* __restrict__ x, const __nv_bfloat16* __res
 	}
 }
 
-// out[r][m] = scale[m] * sum_x in[r][x] exp(-2 pi i m x / T) for m < MX.
-// One warp per row: lanes stride over x, then a warp reduction per mode.
-__global__ void dft_x(const float* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
-                      const float* __restrict__ scale, long long nrows, int T) {
-	__shared__ float2 sh[MAXT];
-	load_tw(sh, tw, T);
-	const int lane = threadIdx.x & 31;
-	const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-	for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < nrows; r += warps) {
-		const float* row = in + r * T;
-		float ar[MX], ai[MX];
+// ------------------------------------------- tensor-core channel products --
+// The per-pixel channel contractions (z = W v, dv = W^T dz, dW = dz v^T) are
+// GEMMs with a 32 x 32 weight or result and the pixels as the long dimension;
+// they run on the tensor cores as mma.sync m16n8k16 with BF16 operands and
+// FP32 accumulation. An FP32 operand is split into a BF16 high part and a
+// BF16 remainder (x = hi + lo to about 2^-16 relative) and the products that
+// matter are summed: with the BF16 weights, which are exact, W hi + W lo; with
+// two FP32 operands, hi hi + hi lo + lo hi. Fragment layouts are those of the
+// PTX ISA for m16n8k16: g = lane / 4, t = lane % 4; A (16 x 16, row major)
+// holds rows g, g + 8 and columns 2t, 2t + 1, 2t + 8, 2t + 9; B (16 x 8) holds
+// rows 2t, 2t + 1, 2t + 8, 2t + 9 of column g; the accumulator holds rows g,
+// g + 8 and columns 2t, 2t + 1.
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+	asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+	             "{%0,%1,%2,%3};\n"
+	             : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+	             : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// two FP32 values (the lower index first) as BF16 pairs: high parts and remainders
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+	const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+	const float2 hf = __bfloat1622float2(h);
+	const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+	hi = *reinterpret_cast<const uint32_t*>(&h);
+	lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+// two BF16 weights as one B-fragment register (the first in the low half)
+__device__ __forceinline__ uint32_t pack_bf16(const __nv_bfloat16* w, size_t i0, size_t i1) {
+	const unsigned short a = *reinterpret_cast<const unsigned short*>(w + i0);
+	const unsigned short b = *reinterpret_cast<const unsigned short*>(w + i1);
+	return (uint32_t)a | ((uint32_t)b << 16);
+}
+
+// The truncated transforms along x are GEMMs too, with the rows as the long
+// dimension and a fixed matrix of twiddles as the other operand, whose
+// BF16-split mma fragments are tabulated once per tile size (dft_frag_kernel):
+//   dft_x:  D[row][2m + q] = sum_x in[row][x] E[x][2m + q], E = cos / -sin(2 pi m x / T)
+//   idft_x: D[row][x] = sum_{m, q} in'[row][2m + q] F[2m + q][x], F = cos / -sin(2 pi m x / T),
+//           in' = scale[m] (Re, Im) of the row's modes
+// Fragment entry (k-step or n-tile, lane) holds the B registers of the high
+// parts and of the remainders.
+
+// fdx: [T/16 k-steps][2 n-tiles][32 lanes], fix: [T/8 n-tiles][32 lanes]
+__global__ void dft_frag_kernel(const float2* __restrict__ tw, int T, uint4* __restrict__ fdx, uint4* __restrict__ fix) {
+	const int nx = T / 16 * 2 * 32, ni = T / 8 * 32;
+	for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nx + ni; e += gridDim.x * blockDim.x) {
+		float v[4];
+		if (e < nx) {
+			const int lane = e & 31, nt = (e >> 5) & 1, ks = e >> 6;
+			const int col = 8 * nt + (lane >> 2), m = col >> 1, q = col & 1, t = lane & 3;
+			const int xs[4] = {16 * ks + 2 * t, 16 * ks + 2 * t + 1, 16 * ks + 2 * t + 8, 16 * ks + 2 * t + 9};
 #pragma unroll
-		for (int m = 0; m < MX; m++) ar[m] = ai[m] = 0.f;
-		for (int x = lane; x < T; x += 32) {
-			const float v = row[x];
+			for (int k = 0; k < 4; k++) {
+				const float2 w = tw[(m * xs[k]) & (T - 1)];
+				v[k] = q ? -w.y : w.x;
+			}
+		} else {
+			const int f = e - nx, lane = f & 31, nt = f >> 5;
+			const int x = 8 * nt + (lane >> 2), t = lane & 3;
+			const float2 w0 = tw[(t * x) & (T - 1)], w4 = tw[((t + 4) * x) & (T - 1)];
+			v[0] = w0.x;
+			v[1] = -w0.y;
+			v[2] = w4.x;
+			v[3] = -w4.y;
+		}
+		uint32_t h0, l0, h1, l1;
+		split2(v[0], v[1], h0, l0);
+		split2(v[2], v[3], h1, l1);
+		const uint4 r = make_uint4(h0, h1, l0, l1);
+		if (e < nx) fdx[e] = r;
+		else fix[e - nx] = r;
+	}
+}
+
+// out[r][m] = scale[m] * sum_x in[r][x] exp(-2 pi i m x / T) for m < MX; one
+// warp per 16 rows
+__global__ void __launch_bounds__(256) dft_x(const float* __restrict__ in, float2* __restrict__ out,
+                                             const uint4* __restrict__ fdx, const float* __restrict__ scale,
+                                             long long nrows, int T) {
+	const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+	const long long ntile = nrows / 16, nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	for (long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntile; tile += nw) {
+		const float* r0 = in + (tile * 16 + g) * T + 2 * t;
+		const float* r8 = r0 + 8LL * T;
+		float acc[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+		for (int ks = 0; ks < T / 16; ks++) {
+			const float2 x0 = *reinterpret_cast<const float2*>(r0 + 16 * ks);
+			const float2 x1 = *reinterpret_cast<const float2*>(r8 + 16 * ks);
+			const float2 x2 = *reinterpret_cast<const float2*>(r0 + 16 * ks + 8);
+			const float2 x3 = *reinterpret_cast<const float2*>(r8 + 16 * ks + 8);
+			uint32_t ah[4], al[4];
+			split2(x0.x, x0.y, ah[0], al[0]);
+			split2(x1.x, x1.y, ah[1], al[1]);
+			split2(x2.x, x2.y, ah[2], al[2]);
+			split2(x3.x, x3.y, ah[3], al[3]);
 #pragma unroll
-			for (int m = 0; m < MX; m++) {
-				const float2 e = sh[(m * x) & (T - 1)];
-				ar[m] += v * e.x;
-				ai[m] -= v * e.y;
+			for (int nt = 0; nt < 2; nt++) {
+				const uint4 f = __ldg(fdx + (ks * 2 + nt) * 32 + lane);
+				const uint32_t bh[2] = {f.x, f.y}, bl[2] = {f.z, f.w};
+				mma_bf16(acc[nt], ah, bh);
+				mma_bf16(acc[nt], ah, bl);
+				mma_bf16(acc[nt], al, bh);
 			}
 		}
-		float xr = 0.f, xi = 0.f;
+		// accumulator columns 2t, 2t + 1 of n-tile nt are (Re, Im) of mode 4 nt + t
 #pragma unroll
-		for (int m = 0; m < MX; m++) {
-			const float sr = warp_sum(ar[m]), si = warp_sum(ai[m]);
-			if (lane == m) {
-				xr = sr;
-				xi = si;
-			}
-		}
-		if (lane < MX) {
-			const float sc = scale ? scale[lane] : 1.f;
-			out[r * MX + lane] = make_float2(xr * sc, xi * sc);
+		for (int nt = 0; nt < 2; nt++) {
+			const int m = 4 * nt + t;
+			const float sc = scale ? scale[m] : 1.f;
+			out[(tile * 16 + g) * MX + m] = make_float2(acc[nt][0] * sc, acc[nt][1] * sc);
+			out[(tile * 16 + g + 8) * MX + m] = make_float2(acc[nt][2] * sc, acc[nt][3] * sc);
 		}
 	}
 }
 
-// out[r][x] (+)= sum_m scale[m] Re(in[r][m] exp(+2 pi i m x / T)); each thread
-// makes four consecutive points of a row from one load of its MX modes
-__global__ void idft_x(const float2* __restrict__ in, float* __restrict__ out, const float2* __restrict__ tw,
-                       const float* __restrict__ scale, long long nrows, int T, int accumulate) {
-	__shared__ float2 sh[MAXT];
-	__shared__ float sc[MX];
-	if (threadIdx.x < MX) sc[threadIdx.x] = scale ? scale[threadIdx.x] : 1.f;
-	load_tw(sh, tw, T);
-	const int q4 = T / 4;
-	const long long n = nrows * q4;
-	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-		const long long r = t / q4;
-		const int x0 = (int)(t - r * q4) * 4;
-		float2 zm[MX];
-#pragma unroll
-		for (int m = 0; m < MX; m++) {
-			const float2 z = in[r * MX + m];
-			zm[m] = make_float2(sc[m] * z.x, sc[m] * z.y);
-		}
-		float acc[4];
-#pragma unroll
-		for (int k = 0; k < 4; k++) {
-			float a = 0.f;
-#pragma unroll
-			for (int m = 0; m < MX; m++) {
-				const float2 e = sh[(m * (x0 + k)) & (T - 1)];
-				a += zm[m].x * e.x - zm[m].y * e.y;
+// out[r][x] (+)= sum_m scale[m] Re(in[r][m] exp(+2 pi i m x / T)); one warp per
+// 16 rows, eight points of each per n-tile
+__global__ void __launch_bounds__(256) idft_x(const float2* __restrict__ in, float* __restrict__ out,
+                                              const uint4* __restrict__ fix, const float* __restrict__ scale,
+                                              long long nrows, int T, int accumulate) {
+	const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+	const float s0 = scale ? scale[t] : 1.f, s4 = scale ? scale[t + 4] : 1.f;
+	const long long ntile = nrows / 16, nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	for (long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntile; tile += nw) {
+		const long long ra = tile * 16 + g, rb = ra + 8;
+		const float2 z0 = in[ra * MX + t], z1 = in[rb * MX + t], z2 = in[ra * MX + t + 4], z3 = in[rb * MX + t + 4];
+		uint32_t ah[4], al[4];
+		split2(s0 * z0.x, s0 * z0.y, ah[0], al[0]);
+		split2(s0 * z1.x, s0 * z1.y, ah[1], al[1]);
+		split2(s4 * z2.x, s4 * z2.y, ah[2], al[2]);
+		split2(s4 * z3.x, s4 * z3.y, ah[3], al[3]);
+		float* oa = out + ra * T + 2 * t;
+		float* ob = out + rb * T + 2 * t;
+		for (int nt = 0; nt < T / 8; nt++) {
+			const uint4 f = __ldg(fix + nt * 32 + lane);
+			const uint32_t bh[2] = {f.x, f.y}, bl[2] = {f.z, f.w};
+			float d[4] = {0.f, 0.f, 0.f, 0.f};
+			mma_bf16(d, ah, bh);
+			mma_bf16(d, ah, bl);
+			mma_bf16(d, al, bh);
+			float2* pa = reinterpret_cast<float2*>(oa + 8 * nt);
+			float2* pb = reinterpret_cast<float2*>(ob + 8 * nt);
+			float2 va = make_float2(d[0], d[1]), vb = make_float2(d[2], d[3]);
+			if (accumulate) {
+				const float2 qa = *pa, qb = *pb;
+				va.x += qa.x;
+				va.y += qa.y;
+				vb.x += qb.x;
+				vb.y += qb.y;
 			}
-			acc[k] = a;
+			*pa = va;
+			*pb = vb;
 		}
-		float4* o4 = reinterpret_cast<float4*>(out + r * T + x0);
-		float4 res = make_float4(acc[0], acc[1], acc[2], acc[3]);
-		if (accumulate) {
-			const float4 p = *o4;
-			res.x += p.x;
-			res.y += p.y;
-			res.z += p.z;
-			res.w += p.w;
-		}
-		*o4 = res;
 	}
 }
 
@@ -254,108 +333,208 @@ __global__ void mix_grad(const float2* __restrict__ X, const float2* __restrict_
 	}
 }
 
-// z = W v + b + s; out = gelu(z) (act) or z. One thread per pixel; W rows are
-// read from shared memory four weights at a time.
-__global__ void __launch_bounds__(128) pointwise_fwd(const float* __restrict__ v, const float* __restrict__ s,
+// z = W v + b + s; out = gelu(z) (act) or z. One warp per 16-pixel tile:
+// D[pixel][out] = sum_in A[pixel][in] B[in][out] with A = v, B = W^T.
+__global__ void __launch_bounds__(128, 4) pointwise_fwd(const float* __restrict__ v, const float* __restrict__ s,
                                                      const __nv_bfloat16* __restrict__ w, int l, float* __restrict__ z,
                                                      float* __restrict__ out, int B, int npix, int act) {
-	__shared__ float4 Ws[C][C / 4];
-	__shared__ float bs[C];
-	float* wsf = reinterpret_cast<float*>(Ws);
-	for (int i = threadIdx.x; i < C * C; i += blockDim.x) wsf[i] = wld(w, off_W(l) + i);
-	for (int i = threadIdx.x; i < C; i += blockDim.x) bs[i] = wld(w, off_b(l) + i);
-	__syncthreads();
-	const long long n = (long long)B * npix;
-	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-		const long long b = t / npix;
-		const long long base = b * C * npix + (t - b * npix);
-		float in[C];
+	const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+	uint32_t bw[4][2][2];
+	float bias[4][2];
 #pragma unroll
-		for (int i = 0; i < C; i++) in[i] = v[base + (long long)i * npix];
-#pragma unroll 4
-		for (int o = 0; o < C; o++) {
-			float acc = bs[o] + s[base + (long long)o * npix];
+	for (int nt = 0; nt < 4; nt++) {
+		const size_t row = off_W(l) + (size_t)(8 * nt + g) * C;
 #pragma unroll
-			for (int q = 0; q < C / 4; q++) {
-				const float4 wq = Ws[o][q];
-				acc += wq.x * in[4 * q] + wq.y * in[4 * q + 1] + wq.z * in[4 * q + 2] + wq.w * in[4 * q + 3];
+		for (int ks = 0; ks < 2; ks++) {
+			bw[nt][ks][0] = pack_bf16(w, row + 16 * ks + 2 * t, row + 16 * ks + 2 * t + 1);
+			bw[nt][ks][1] = pack_bf16(w, row + 16 * ks + 2 * t + 8, row + 16 * ks + 2 * t + 9);
+		}
+		bias[nt][0] = wld(w, off_b(l) + 8 * nt + 2 * t);
+		bias[nt][1] = wld(w, off_b(l) + 8 * nt + 2 * t + 1);
+	}
+	const int tpi = npix / 16;
+	const long long ntile = (long long)B * tpi;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	for (long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntile; tile += nw) {
+		const long long b = tile / tpi;
+		const long long base = b * C * npix + (tile - b * tpi) * 16;
+		uint32_t ah[2][4], al[2][4];
+#pragma unroll
+		for (int ks = 0; ks < 2; ks++) {
+			const float* c0 = v + base + (long long)(16 * ks + 2 * t) * npix;
+			const float* c1 = c0 + npix;
+			const float* c8 = c0 + 8LL * npix;
+			const float* c9 = c8 + npix;
+			split2(c0[g], c1[g], ah[ks][0], al[ks][0]);
+			split2(c0[g + 8], c1[g + 8], ah[ks][1], al[ks][1]);
+			split2(c8[g], c9[g], ah[ks][2], al[ks][2]);
+			split2(c8[g + 8], c9[g + 8], ah[ks][3], al[ks][3]);
+		}
+#pragma unroll
+		for (int nt = 0; nt < 4; nt++) {
+			const long long o0 = base + (long long)(8 * nt + 2 * t) * npix, o1 = o0 + npix;
+			float d[4] = {bias[nt][0] + s[o0 + g], bias[nt][1] + s[o1 + g], bias[nt][0] + s[o0 + g + 8],
+			              bias[nt][1] + s[o1 + g + 8]};
+#pragma unroll
+			for (int ks = 0; ks < 2; ks++) {
+				mma_bf16(d, ah[ks], bw[nt][ks]);
+				mma_bf16(d, al[ks], bw[nt][ks]);
 			}
-			if (z) z[base + (long long)o * npix] = acc;
-			out[base + (long long)o * npix] = act ? gelu(acc) : acc;
+			if (z) {
+				z[o0 + g] = d[0];
+				z[o1 + g] = d[1];
+				z[o0 + g + 8] = d[2];
+				z[o1 + g + 8] = d[3];
+			}
+			out[o0 + g] = act ? gelu(d[0]) : d[0];
+			out[o1 + g] = act ? gelu(d[1]) : d[1];
+			out[o0 + g + 8] = act ? gelu(d[2]) : d[2];
+			out[o1 + g + 8] = act ? gelu(d[3]) : d[3];
 		}
 	}
 }
 
-// dz = dout * g'(z) (also the gradient of the spectral branch); dv = W^T dz,
-// with W held transposed in shared memory and read four weights at a time
-__global__ void __launch_bounds__(128) pointwise_bwd(const float* __restrict__ z, const float* __restrict__ dout,
+// dz = dout * g'(z) (also the gradient of the spectral branch); dv = W^T dz:
+// D[pixel][in] = sum_out A[pixel][out] B[out][in] with A = dz, B = W.
+__global__ void __launch_bounds__(128, 4) pointwise_bwd(const float* __restrict__ z, const float* __restrict__ dout,
                                                      const __nv_bfloat16* __restrict__ w, int l, float* __restrict__ dz,
                                                      float* __restrict__ dv, int B, int npix, int act) {
-	__shared__ float4 WT[C][C / 4]; // WT[i][o / 4] = W[o .. o+3][i]
-	float* wtf = reinterpret_cast<float*>(WT);
-	for (int k = threadIdx.x; k < C * C; k += blockDim.x) {
-		const int o = k / C, i = k % C;
-		wtf[i * C + o] = wld(w, off_W(l) + k);
-	}
-	__syncthreads();
-	const long long n = (long long)B * npix;
-	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-		const long long b = t / npix;
-		const long long base = b * C * npix + (t - b * npix);
-		float d[C];
+	const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+	uint32_t bw[4][2][2];
 #pragma unroll
-		for (int o = 0; o < C; o++) {
-			const float g = dout[base + (long long)o * npix];
-			d[o] = act ? g * gelu_d(z[base + (long long)o * npix]) : g;
-			dz[base + (long long)o * npix] = d[o];
+	for (int nt = 0; nt < 4; nt++) {
+		const size_t col = off_W(l) + 8 * nt + g; // W[o][i = 8 nt + g] at col + o C
+#pragma unroll
+		for (int ks = 0; ks < 2; ks++) {
+			const int o = 16 * ks + 2 * t;
+			bw[nt][ks][0] = pack_bf16(w, col + (size_t)o * C, col + (size_t)(o + 1) * C);
+			bw[nt][ks][1] = pack_bf16(w, col + (size_t)(o + 8) * C, col + (size_t)(o + 9) * C);
 		}
-#pragma unroll 4
-		for (int i = 0; i < C; i++) {
-			float acc = 0.f;
+	}
+	const int tpi = npix / 16;
+	const long long ntile = (long long)B * tpi;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	for (long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntile; tile += nw) {
+		const long long b = tile / tpi;
+		const long long base = b * C * npix + (tile - b * tpi) * 16;
+		uint32_t ah[2][4], al[2][4];
 #pragma unroll
-			for (int q = 0; q < C / 4; q++) {
-				const float4 wq = WT[i][q];
-				acc += wq.x * d[4 * q] + wq.y * d[4 * q + 1] + wq.z * d[4 * q + 2] + wq.w * d[4 * q + 3];
+		for (int ks = 0; ks < 2; ks++) {
+			float dd[8];
+			const int och[4] = {16 * ks + 2 * t, 16 * ks + 2 * t + 1, 16 * ks + 2 * t + 8, 16 * ks + 2 * t + 9};
+#pragma unroll
+			for (int q = 0; q < 4; q++)
+#pragma unroll
+				for (int h = 0; h < 2; h++) {
+					const long long i = base + (long long)och[q] * npix + g + 8 * h;
+					const float gv = dout[i];
+					const float d = act ? gv * gelu_d(z[i]) : gv;
+					dz[i] = d;
+					dd[2 * q + h] = d;
+				}
+			// a0 (g; o, o+1), a1 (g+8; o, o+1), a2 (g; o+8, o+9), a3 (g+8; o+8, o+9)
+			split2(dd[0], dd[2], ah[ks][0], al[ks][0]);
+			split2(dd[1], dd[3], ah[ks][1], al[ks][1]);
+			split2(dd[4], dd[6], ah[ks][2], al[ks][2]);
+			split2(dd[5], dd[7], ah[ks][3], al[ks][3]);
+		}
+#pragma unroll
+		for (int nt = 0; nt < 4; nt++) {
+			float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+			for (int ks = 0; ks < 2; ks++) {
+				mma_bf16(d, ah[ks], bw[nt][ks]);
+				mma_bf16(d, al[ks], bw[nt][ks]);
 			}
-			dv[base + (long long)i * npix] = acc;
+			const long long i0 = base + (long long)(8 * nt + 2 * t) * npix, i1 = i0 + npix;
+			dv[i0 + g] = d[0];
+			dv[i1 + g] = d[1];
+			dv[i0 + g + 8] = d[2];
+			dv[i1 + g + 8] = d[3];
 		}
 	}
 }
 
-// dW[o][i] += sum_p dz[o][p] v[i][p], db[o] += sum_p dz[o][p]: a C x C product
-// over all pixels. Each block stages 64-pixel tiles of dz and v in shared
-// memory; thread t owns W entries (o = t / 8, i = 4 (t % 8) .. +3).
-constexpr int WG_TILE = 64;
-__global__ void __launch_bounds__(256) weight_grad(const float* __restrict__ dz, const float* __restrict__ v,
-                                                   float* __restrict__ gW, float* __restrict__ gb, int B, int npix) {
-	__shared__ float sd[C][WG_TILE + 1];
-	__shared__ float sv[C][WG_TILE + 1];
-	const int o = threadIdx.x >> 3, i0 = (threadIdx.x & 7) * 4;
-	float acc[4] = {0.f, 0.f, 0.f, 0.f}, accb = 0.f;
-	const int tiles_per_image = npix / WG_TILE;
-	const long long ntiles = (long long)B * tiles_per_image;
-	for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-		const long long b = tile / tiles_per_image;
-		const int p0 = (int)(tile - b * tiles_per_image) * WG_TILE;
-		__syncthreads();
-		for (int e = threadIdx.x; e < C * WG_TILE; e += blockDim.x) {
-			const int c = e / WG_TILE, p = e % WG_TILE;
-			const long long gi = (b * C + c) * (long long)npix + p0 + p;
-			sd[c][p] = dz[gi];
-			sv[c][p] = v[gi];
-		}
-		__syncthreads();
-#pragma unroll 8
-		for (int p = 0; p < WG_TILE; p++) {
-			const float d = sd[o][p];
+// dW[o][i] += sum_p dz[o][p] v[i][p], db[o] += sum_p dz[o][p]: D[o][i] = sum_p
+// A[o][p] B[p][i] with A = dz, B = v^T, 16 pixels per step; each warp sums its
+// tiles, the block adds its warps in shared memory, then one atomic per entry.
+constexpr int WG_THREADS = 256;
+__global__ void __launch_bounds__(WG_THREADS) weight_grad(const float* __restrict__ dz, const float* __restrict__ v,
+                                                          float* __restrict__ gW, float* __restrict__ gb, int B,
+                                                          int npix) {
+	__shared__ float sW[C * C];
+	__shared__ float sb[C];
+	for (int i = threadIdx.x; i < C * C; i += blockDim.x) sW[i] = 0.f;
+	if (threadIdx.x < C) sb[threadIdx.x] = 0.f;
+	__syncthreads();
+	const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+	float acc[2][4][4];
 #pragma unroll
-			for (int k = 0; k < 4; k++) acc[k] += d * sv[i0 + k][p];
-			accb += d;
+	for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+		for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+			for (int k = 0; k < 4; k++) acc[mt][nt][k] = 0.f;
+	float bsum[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+	const int tpi = npix / 16;
+	const long long ntile = (long long)B * tpi;
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	for (long long tile = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < ntile; tile += nw) {
+		const long long b = tile / tpi;
+		const long long base = b * C * npix + (tile - b * tpi) * 16 + 2 * t;
+		uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+		for (int mt = 0; mt < 2; mt++) {
+			const float* r0 = dz + base + (long long)(16 * mt + g) * npix;
+			const float* r8 = r0 + 8LL * npix;
+			const float2 x0 = *reinterpret_cast<const float2*>(r0), x1 = *reinterpret_cast<const float2*>(r8);
+			const float2 x2 = *reinterpret_cast<const float2*>(r0 + 8), x3 = *reinterpret_cast<const float2*>(r8 + 8);
+			split2(x0.x, x0.y, ah[mt][0], al[mt][0]);
+			split2(x1.x, x1.y, ah[mt][1], al[mt][1]);
+			split2(x2.x, x2.y, ah[mt][2], al[mt][2]);
+			split2(x3.x, x3.y, ah[mt][3], al[mt][3]);
+			bsum[mt][0] += (x0.x + x0.y) + (x2.x + x2.y);
+			bsum[mt][1] += (x1.x + x1.y) + (x3.x + x3.y);
 		}
+#pragma unroll
+		for (int nt = 0; nt < 4; nt++) {
+			const float* r = v + base + (long long)(8 * nt + g) * npix;
+			const float2 y0 = *reinterpret_cast<const float2*>(r), y1 = *reinterpret_cast<const float2*>(r + 8);
+			split2(y0.x, y0.y, bh[nt][0], bl[nt][0]);
+			split2(y1.x, y1.y, bh[nt][1], bl[nt][1]);
+		}
+#pragma unroll
+		for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+			for (int nt = 0; nt < 4; nt++) {
+				mma_bf16(acc[mt][nt], ah[mt], bh[nt]);
+				mma_bf16(acc[mt][nt], ah[mt], bl[nt]);
+				mma_bf16(acc[mt][nt], al[mt], bh[nt]);
+			}
 	}
 #pragma unroll
-	for (int k = 0; k < 4; k++) atomicAdd(&gW[o * C + i0 + k], acc[k]);
-	if ((threadIdx.x & 7) == 0) atomicAdd(&gb[o], accb);
+	for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+		for (int nt = 0; nt < 4; nt++) {
+			const int o = 16 * mt + g, i = 8 * nt + 2 * t;
+			atomicAdd(&sW[o * C + i], acc[mt][nt][0]);
+			atomicAdd(&sW[o * C + i + 1], acc[mt][nt][1]);
+			atomicAdd(&sW[(o + 8) * C + i], acc[mt][nt][2]);
+			atomicAdd(&sW[(o + 8) * C + i + 1], acc[mt][nt][3]);
+		}
+	// bias: the four lanes of a group hold disjoint pixels of the same rows
+#pragma unroll
+	for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+		for (int h = 0; h < 2; h++) {
+			float x = bsum[mt][h];
+			x += __shfl_xor_sync(0xffffffffu, x, 1);
+			x += __shfl_xor_sync(0xffffffffu, x, 2);
+			if (t == 0) atomicAdd(&sb[16 * mt + g + 8 * h], x);
+		}
+	__syncthreads();
+	for (int i = threadIdx.x; i < C * C; i += blockDim.x) atomicAdd(&gW[i], sW[i]);
+	if (threadIdx.x < C) atomicAdd(&gb[threadIdx.x], sb[threadIdx.x]);
 }
 
 // y = x + Q v + q; with a target also loss += sum (y - t)^2 / n and dy = 2 (y - t) / n
@@ -595,6 +774,8 @@ struct pfcg_fno {
 	float* av = nullptr;
 	long long adam_t = 0;
 	float2* tw = nullptr;        // twiddles of the tile size
+	uint4* fdx = nullptr;        // mma fragments of the truncated x transforms (dft_frag_kernel)
+	uint4* fix = nullptr;
 	float* sx = nullptr;         // per-kx weights of the truncated irfft2: (kx ? 2 : 1) / T^2
 	float* v[L + 1] = {};        // layer inputs (v[L] feeds the projection)
 	float* z[L] = {};            // pre-activations
@@ -639,12 +820,12 @@ int forward(pfcg_fno* f, const float* x, int B, const float* target, bool train)
 	lift_fwd<<<grid_for((long long)B * npix, 256), 256, 0, st>>>(x, f->w, f->v[0], B, npix);
 	f->launches++;
 	for (int l = 0; l < L; l++) {
-		dft_x<<<grid_for(rows * 32, 256), 256, 0, st>>>(f->v[l], f->A, f->tw, nullptr, rows, T);
+		dft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->v[l], f->A, f->fdx, nullptr, rows, T);
 		dft_y<<<planes_grid(planes), 128, 0, st>>>(f->A, f->X[l], f->tw, planes, T, 0);
 		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->w, l, B, 0);
 		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Y, f->Bq, f->tw, planes, T, 1);
-		idft_x<<<grid_for(rows * T / 4, 256), 256, 0, st>>>(f->Bq, f->s, f->tw, f->sx, rows, T, 0);
-		pointwise_fwd<<<grid_for((long long)B * npix, 128), 128, 0, st>>>(f->v[l], f->s, f->w, l, train ? f->z[l] : nullptr,
+		idft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->Bq, f->s, f->fix, f->sx, rows, T, 0);
+		pointwise_fwd<<<grid_for((long long)B * npix / 16 * 32, 128), 128, 0, st>>>(f->v[l], f->s, f->w, l, train ? f->z[l] : nullptr,
 		                                                                    f->v[l + 1], B, npix, l < L - 1);
 		f->launches += 6;
 	}
@@ -661,7 +842,7 @@ int backward(pfcg_fno* f, const float* x, int B) {
 	const long long rows = (long long)B * C * T, planes = (long long)B * C;
 	cudaStream_t st = f->stream;
 	const dim3 cg(std::min(grid_for((long long)B * npix, 256), 64), C);
-	const int wg = std::min(grid_for((long long)B * npix / WG_TILE, 1), 148 * 4);
+	const int wg = std::min(grid_for((long long)B * npix / 16 / (WG_THREADS / 32), 1), 148 * 4);
 	FCK(cudaMemsetAsync(f->g, 0, sizeof(float) * NPARAM, st));
 	// projection: dQ[j][c] = sum v_L[c] dy[j], dq[j] = sum dy[j], dv_L = Q^T dy
 	channel_grad<<<cg, 256, 0, st>>>(f->v[L], f->dy, f->g + OFF_Q, 1, C, nullptr, B, npix);
@@ -669,16 +850,16 @@ int backward(pfcg_fno* f, const float* x, int B) {
 	proj_bwd<<<grid_for((long long)B * npix, 256), 256, 0, st>>>(f->dy, f->w, f->dv, B, npix);
 	f->launches += 3;
 	for (int l = L - 1; l >= 0; l--) {
-		pointwise_bwd<<<grid_for((long long)B * npix, 128), 128, 0, st>>>(f->z[l], f->dv, f->w, l, f->dz, f->dv2, B, npix,
+		pointwise_bwd<<<grid_for((long long)B * npix / 16 * 32, 128), 128, 0, st>>>(f->z[l], f->dv, f->w, l, f->dz, f->dv2, B, npix,
 		                                                                    l < L - 1);
-		weight_grad<<<wg, 256, 0, st>>>(f->dz, f->v[l], f->g + off_W(l), f->g + off_b(l), B, npix);
+		weight_grad<<<wg, WG_THREADS, 0, st>>>(f->dz, f->v[l], f->g + off_W(l), f->g + off_b(l), B, npix);
 		// spectral branch, in reverse
-		dft_x<<<grid_for(rows * 32, 256), 256, 0, st>>>(f->dz, f->Bq, f->tw, f->sx, rows, T);
+		dft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->dz, f->Bq, f->fdx, f->sx, rows, T);
 		dft_y<<<planes_grid(planes), 128, 0, st>>>(f->Bq, f->Y, f->tw, planes, T, 0);
 		mix_grad<<<grid_for((long long)C * C * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->g, l, B);
 		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->Y, f->Bq, f->w, l, B, 1);
 		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Bq, f->A, f->tw, planes, T, 1);
-		idft_x<<<grid_for(rows * T / 4, 256), 256, 0, st>>>(f->A, f->dv2, f->tw, nullptr, rows, T, 1);
+		idft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->A, f->dv2, f->fix, nullptr, rows, T, 1);
 		f->launches += 8;
 		std::swap(f->dv, f->dv2);
 	}
@@ -764,6 +945,8 @@ int pfcg_fno_create(int tile, int max_batch, pfcg_fno** out) {
 	add((void**)&f->am, sizeof(float) * NPARAM);
 	add((void**)&f->av, sizeof(float) * NPARAM);
 	add((void**)&f->tw, sizeof(float2) * tile);
+	add((void**)&f->fdx, sizeof(uint4) * (tile / 16) * 2 * 32);
+	add((void**)&f->fix, sizeof(uint4) * (tile / 8) * 32);
 	add((void**)&f->sx, sizeof(float) * MX);
 	for (int l = 0; l <= L; l++) add((void**)&f->v[l], sizeof(float) * nv);
 	for (int l = 0; l < L; l++) add((void**)&f->z[l], sizeof(float) * nv);
@@ -789,7 +972,8 @@ int pfcg_fno_create(int tile, int max_batch, pfcg_fno** out) {
 	for (int m = 0; m < MX; m++) sc[m] = (m == 0 ? 1.f : 2.f) / (float)npix;
 	e = cudaMemcpyAsync(f->sx, sc, sizeof(sc), cudaMemcpyHostToDevice, f->stream);
 	twiddle_kernel<<<1, 256, 0, f->stream>>>(f->tw, tile);
-	f->launches++;
+	dft_frag_kernel<<<(tile * 8 + 255) / 256, 256, 0, f->stream>>>(f->tw, tile, f->fdx, f->fix);
+	f->launches += 2;
 	for (size_t i = 0; i < 5 && e == cudaSuccess; i++) e = cudaMemsetAsync(*bufs[i], 0, sizes[i], f->stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
 	if (e == cudaSuccess) e = cudaGetLastError();
