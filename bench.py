@@ -140,20 +140,25 @@ def traffic_from_profiles(kernel: str, workload_name: str):
         return None
 
 
-def cpu_baseline(N: int, U: int, rank: int, steps: int, warmup: int = 1):
+def cpu_baseline(N: int, U: int, rank: int, steps: int, warmup: int = 1, case=None):
     """The reference solver's step (demos/honey/pfc-relax.c over the project FFT
     shim, all host threads) timed on a bounded sample of the same workload:
-    `warmup` untimed steps, then `steps` timed ones."""
+    `warmup` untimed steps, then `steps` timed ones. case = (parameter dict,
+    dx, dy, fields, dt, c) replaces the heterostructure workload."""
     exe = os.path.join(ROOT, "oracle", "_ref", "pfc-relax-bench")
     if not os.path.exists(exe):
         return None
-    pd, dx, dy, f = workload(N, rank)
+    if case is None:
+        pd, dx, dy, f = workload(N, rank)
+        dt, c = 0.25, 1.0
+    else:
+        pd, dx, dy, f, dt, c = case
     with tempfile.TemporaryDirectory() as d:
         ins = ["in%d.n" % u for u in range(U)]
         for u in range(U):
             nfile.write_n_header_only(os.path.join(d, ins[u]), N, N, dx, dy)
         nfile.write_input(os.path.join(d, "x.in"), ins, ["o%d" % u for u in range(U)], Tprint=10 ** 9,
-                          Twrite=10 ** 9, params=pd, c=1.0, tend=10 ** 6, dx=dx, dy=dy, dt=0.25)
+                          Twrite=10 ** 9, params=pd, c=c, tend=10 ** 6, dx=dx, dy=dy, dt=dt)
         np.ascontiguousarray(f, dtype="<f8").tofile(os.path.join(d, "fields.bin"))
         env = dict(os.environ)
         threads = os.cpu_count() or 1
@@ -168,6 +173,48 @@ def cpu_baseline(N: int, U: int, rank: int, steps: int, warmup: int = 1):
             "sample": "%d steps of %dx%d U=%d after %d warm-up steps; reference step() over the project FFT shim "
                       "(not FFTW), %d OpenMP threads in the FFT, pointwise loops single-threaded"
                       % (res["steps"], N, N, U, warmup, res["threads"])}
+
+
+def config_cases():
+    """The single-field configurations beside the headline: C1 (512^2 honeycomb
+    from noise, dt = 1) and C2 (2048^2 32-grain polycrystal, dt = 1), both
+    with dx = dy = pi/4; (name, N, parameter dict, dx, fields, dt, c)."""
+    pd = P.honeycomb_1c(-0.25)
+    dx = math.pi / 4
+    return [("c1_honeycomb_512", 512, pd, dx, synth.noise_state(512, 512, 0.25, 0.05, 0)[None], 1.0, 1.0),
+            ("c2_polycrystal_2048", 2048, pd, dx, synth.polycrystal(2048, 2048, dx, dx, 32, 0.25, -0.4, 0.01, 0)[None],
+             1.0, 1.0)]
+
+
+def configs_record(steps: int, warmup: int, cpu: bool) -> dict:
+    """Steps/s of C1 and C2 on the GPU in both precisions (CUDA events on the
+    handle's stream), and the reference's CPU step on bounded samples."""
+    import torch
+
+    out = {}
+    for name, N, pd, dx, f0, dt, c in config_cases():
+        params = P.make_params(pd, c, dt)
+        rec = {"grid": [N, N], "U": 1}
+        for prec in ("fp32", "fp64"):
+            with lib.Relaxation(params, N, N, dx, dx, prec) as r:
+                r.upload(f0)
+                r.step(warmup)
+                st = torch.cuda.ExternalStream(r.stream)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(st)
+                r.step(steps)
+                e1.record(st)
+                torch.cuda.synchronize()
+                rec[prec + "_steps_per_s"] = steps * 1000.0 / e0.elapsed_time(e1)
+        if cpu:
+            k = 20 if N <= 512 else 5
+            cb = cpu_baseline(N, 1, 0, k, 1, case=(pd, dx, dx, f0, dt, c))
+            if cb and "error" not in cb:
+                rec["reference_cpu_steps_per_s"] = cb["value"]
+                rec["reference_cpu_sample"] = cb["sample"]
+        out[name] = rec
+    return out
 
 
 def batch_problems(seed: int = 7, n: int = 96):
@@ -420,6 +467,7 @@ def main():
     ap.add_argument("--no-cufft", action="store_true", help="skip the cuFFT reference timing")
     ap.add_argument("--batch", action="store_true", help="the batched workload (96 mixed problems) instead")
     ap.add_argument("--no-batch", action="store_true", help="leave the batched workload out of the default line")
+    ap.add_argument("--no-configs", action="store_true", help="leave the C1/C2 timings out of the default line")
     ap.add_argument("--batch-steps", type=int, default=200, help="timed steps of the batch record")
     ap.add_argument("--ttr", action="store_true", help="time to relaxed: plain FP64, plain FP32, warm-started FP32")
     ap.add_argument("--ttr-max-steps", type=int, default=80000)
@@ -587,6 +635,8 @@ def main():
                         "fave": r64["fave"], "rel_dF_vs_fp32": abs(res["fave"] - r64["fave"]) / abs(r64["fave"])}
     if acc:
         line["accuracy_fp32_vs_fp64"] = acc
+    if rank == 0 and world == 1 and not args.no_configs and main_p == "fp32":
+        line["configs"] = configs_record(max(args.steps, 50), max(3, args.warmup), not args.no_cpu)
     if rank == 0 and world == 1 and not args.no_batch and main_p == "fp32":
         line["batch"] = batch_record(args.batch_steps, max(3, args.warmup))
     if rank == 0 and world == 1 and not args.no_ttr and main_p == "fp32":
