@@ -251,7 +251,8 @@ int choose_layout(pfcg_handle* h, int nsm) {
 
 // Per-pass twiddle table of a compile-time length N (the layout of fft_core.cuh's
 // CtPlan): passes of radix rmain with the tail radix second; pass p > 0 contributes
-// entries [(r - 1) * Ns + jm] = exp(-2 pi i r jm / (Ns R)).
+// entries [q * Ns + jm] = exp(-2 pi i r_q jm / (Ns R)) with r_q = q + 1, or for
+// radix 16 r_q in {1, 2, 3, 4, 8, 12} (ct_twiddle makes the other powers).
 template <typename T> int upload_ct_twiddles(pfcg_handle* h, int N, int rmain, void** dst) {
 	// N = rmain^A * tail; the tail radix is the second pass (fft_core.cuh, CtPlan)
 	std::vector<int> radix;
@@ -265,9 +266,12 @@ template <typename T> int upload_ct_twiddles(pfcg_handle* h, int N, int rmain, v
 	int Ns = 1;
 	for (size_t p = 0; p < radix.size(); p++) {
 		const int R = radix[p];
+		static const int pow16[6] = {1, 2, 3, 4, 8, 12};
+		const int nq = R == 16 ? 6 : R - 1;
 		if (p > 0)
-			for (int r = 1; r < R; r++)
+			for (int q = 0; q < nq; q++)
 				for (int jm = 0; jm < Ns; jm++) {
+					const int r = R == 16 ? pow16[q] : q + 1;
 					const double a = -2.0 * PI * (double)r * (double)jm / ((double)Ns * R);
 					cplx<T> w;
 					w.x = (T)std::cos(a);

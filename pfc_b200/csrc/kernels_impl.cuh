@@ -350,8 +350,18 @@ __device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm,
 		const int k = tid + it * NT;
 		if (k >= H) break;
 		cplx<T> y[CH];
+		if constexpr (sizeof(T) == 4 && RC == 2) {
+			// both rows of a field at k are one 16-byte word
 #pragma unroll
-		for (int c = 0; c < CH; c++) y[c] = a.work[(c % U) * a.wstride + tofs + (long long)k * RC + c / U];
+			for (int u = 0; u < U; u++) {
+				const float4 q = *reinterpret_cast<const float4*>(a.work + u * a.wstride + tofs + (long long)k * RC);
+				y[u] = mk<T>(q.x, q.y);
+				y[U + u] = mk<T>(q.z, q.w);
+			}
+		} else {
+#pragma unroll
+			for (int c = 0; c < CH; c++) y[c] = a.work[(c % U) * a.wstride + tofs + (long long)k * RC + c / U];
+		}
 		const bool selfc = (k == 0) || (2 * k == NC);
 #pragma unroll
 		for (int p = 0; p < P; p++) {
@@ -425,8 +435,15 @@ __device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm,
 			zz[2 * p] = mk<T>(half * (Ck.x + Cm.x), half * (Ck.y - Cm.y));
 			zz[2 * p + 1] = mk<T>(half * (Ck.y + Cm.y), half * (Cm.x - Ck.x));
 		}
+		if constexpr (sizeof(T) == 4 && RC == 2) {
 #pragma unroll
-		for (int c = 0; c < CH; c++) a.work[(c % U) * a.wstride + tofs + (long long)k * RC + c / U] = zz[c];
+			for (int u = 0; u < U; u++)
+				*reinterpret_cast<float4*>(a.work + u * a.wstride + tofs + (long long)k * RC) =
+				    make_float4(zz[u].x, zz[u].y, zz[U + u].x, zz[U + u].y);
+		} else {
+#pragma unroll
+			for (int c = 0; c < CH; c++) a.work[(c % U) * a.wstride + tofs + (long long)k * RC + c / U] = zz[c];
+		}
 	}
 	double acc[U];
 #pragma unroll
