@@ -361,7 +361,7 @@ template <int N, int RM> struct CtPlan {
 // v[r] *= w^r for r = 1 .. R-1, w = exp(SIGN 2 pi i jm / (NS R)); twj points at
 // the pass's table entry for jm (layout above).
 template <int R, int NS, int SIGN, typename T>
-__device__ __forceinline__ void ct_twiddle(cplx<T>* v, const cplx<T>* twj) {
+__host__ __device__ __forceinline__ void ct_twiddle(cplx<T>* v, const cplx<T>* twj) {
 	if constexpr (R == 16) {
 		cplx<T> b[6]; // w^1, w^2, w^3, w^4, w^8, w^12
 #pragma unroll

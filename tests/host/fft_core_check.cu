@@ -36,7 +36,7 @@ template <int N, int RM> static void check_plan() {
 	using PL = CtPlan<N, RM>;
 	int prod = 1, tw = 0;
 	for (int p = 0; p < PL::NPASS; p++) {
-		if (p > 0) tw += (PL::radix(p) - 1) * PL::ns(p);
+		if (p > 0) tw += PL::twcnt(PL::radix(p)) * PL::ns(p);
 		prod *= PL::radix(p);
 	}
 	const bool ok = prod == N && PL::FUSABLE && PL::radix(0) == RM && PL::radix(PL::NPASS - 1) == RM &&
@@ -46,7 +46,33 @@ template <int N, int RM> static void check_plan() {
 	            ok ? "ok" : "FAIL");
 }
 
+// ct_twiddle on a radix-16 pass (powers 1, 2, 3, 4, 8, 12 tabulated, the rest
+// as products) against the direct powers exp(SIGN 2 pi i r jm / (NS 16))
+template <int NS, int SIGN> static void check_twiddle16() {
+	cplx<double> tab[6 * NS];
+	const int pw[6] = {1, 2, 3, 4, 8, 12};
+	for (int q = 0; q < 6; q++)
+		for (int jm = 0; jm < NS; jm++) {
+			const double a = -2.0 * M_PI * pw[q] * jm / (NS * 16.0);
+			tab[q * NS + jm] = mk<double>(std::cos(a), std::sin(a));
+		}
+	double err = 0;
+	for (int jm = 0; jm < NS; jm++) {
+		cplx<double> v[16];
+		for (int r = 0; r < 16; r++) v[r] = mk<double>(1.0, 0.0);
+		ct_twiddle<16, NS, SIGN, double>(v, tab + jm);
+		for (int r = 1; r < 16; r++) {
+			const double a = SIGN * 2.0 * M_PI * r * jm / (NS * 16.0);
+			err = std::fmax(err, std::hypot(v[r].x - std::cos(a), v[r].y - std::sin(a)));
+		}
+	}
+	const bool ok = err < 1e-14;
+	failures += !ok;
+	std::printf("twiddle16 NS %d sign %+d max error %.2e %s\n", NS, SIGN, err, ok ? "ok" : "FAIL");
+}
+
 int main() {
+	check_twiddle16<16, -1>(); check_twiddle16<16, 1>(); check_twiddle16<256, -1>(); check_twiddle16<256, 1>();
 	check_dft<2, -1>(); check_dft<2, 1>();
 	check_dft<3, -1>(); check_dft<3, 1>();
 	check_dft<4, -1>(); check_dft<4, 1>();

@@ -1,6 +1,6 @@
 """The in-register DFTs (radix 2-8 and 16, including the prime-factor radix 6
-of the 1536-point tail pass) and the compile-time pass plans of every
-specialised length, checked on the CPU: tests/host/fft_core_check.cu compiles
+of the 1536-point tail pass), the radix-16 twiddle powers built from six
+tabulated ones, and the compile-time pass plans of every specialised length, checked on the CPU: tests/host/fft_core_check.cu compiles
 fft_core.cuh's host-and-device code for the host with nvcc and compares each
 DFT with a direct FP64 sum."""
 import os
@@ -21,4 +21,4 @@ def test_dfts_and_plans_on_host(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert out.returncode == 0, out.stdout
     lines = out.stdout.strip().splitlines()
-    assert len(lines) == 26 and all(l.endswith("ok") for l in lines), out.stdout
+    assert len(lines) == 30 and all(l.endswith("ok") for l in lines), out.stdout
