@@ -9,6 +9,8 @@
 //                   smoothing terms by Parseval in k space)
 //   pfcg_optimize   optimize :1251-1290
 //   pfcg_download   the m[u] written by write_data :767-815
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -72,6 +74,8 @@ struct pfcg_handle {
 	double* d_fields = nullptr; // f(r) work fields
 	double* d_part = nullptr;   // partial sums of the field means
 	int regio = 1;              // y-pass register ends (PFCG_YPASS_REGIO=0: load/store phases through shared memory)
+	void* tmap = nullptr;       // device copy of the y-pass's TMA tensor map over `work` (null: plain loads)
+	int tma_tiles = 0;          // row tiles per TMA box
 	long long launches = 0;
 	// per-kernel timing (pfcg_set_profiling)
 	bool profiling = false;
@@ -298,6 +302,52 @@ template <typename T> int upload_twiddles(pfcg_handle* h, int n, void** dst) {
 	return 0;
 }
 
+// The y-pass's TMA tensor map (FP32 specialised y-pass with register ends):
+// `work` as a 4-D tensor of 8-byte complex elements [field][tile][kx][row] with
+// boxes of (R rows, CC columns, tb tiles, 1 field). A box starts on a 16-byte
+// multiple (R * 8 bytes, a multiple of 16, is the innermost extent) and lands
+// on a 128-byte multiple of shared memory. PFCG_TMA=0 in the environment keeps
+// the plain loads. Without a driver entry point the plain loads are used.
+int setup_tma(pfcg_handle* h) {
+	const char* env = std::getenv("PFCG_TMA");
+	if (env && env[0] == '0') return 0;
+	if (h->prec != PFCG_FP32 || !h->cys.spec || h->cys.spec == 1 || !h->regio || h->U > 2) return 0;
+	if (!spec_y_regio(false, h->U, h->Ny)) return 0;
+	const int R = h->geom.R, CC = h->geom.CC, ntile = h->Ny / R;
+	const size_t el = sizeof(float2);
+	if ((R * el) % 16 != 0 || CC > 256 || R > 256) return 0;
+	int tb = 0;
+	for (int t = std::min(256, ntile); t >= 1; t--)
+		if (ntile % t == 0 && (t * CC * R * el) % 128 == 0) {
+			tb = t;
+			break;
+		}
+	if (!tb) return 0;
+	static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+	if (!encode) {
+		cudaDriverEntryPointQueryResult q;
+		void* fn = nullptr;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn) {
+			cudaGetLastError();
+			return 0;
+		}
+		encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+	}
+	CUtensorMap tm;
+	cuuint64_t dims[4] = {(cuuint64_t)R, (cuuint64_t)h->H, (cuuint64_t)ntile, (cuuint64_t)h->U};
+	cuuint64_t strides[3] = {(cuuint64_t)(R * el), (cuuint64_t)h->H * R * el, (cuuint64_t)h->H * h->Ny * el};
+	cuuint32_t box[4] = {(cuuint32_t)R, (cuuint32_t)CC, (cuuint32_t)tb, 1};
+	cuuint32_t es[4] = {1, 1, 1, 1};
+	if (encode(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, h->work, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+	           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+	    CUDA_SUCCESS)
+		return 0;
+	CK(h, cudaMalloc(&h->tmap, sizeof(CUtensorMap)));
+	CK(h, cudaMemcpy(h->tmap, &tm, sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+	h->tma_tiles = tb;
+	return 0;
+}
+
 Model to_model(const pfcg_params* p) {
 	Model m{};
 	m.U = p->U;
@@ -376,6 +426,9 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.m = h->model;
 	a.g = h->geom;
 	a.regio = h->regio;
+	a.tmap = h->tmap;
+	a.tma_tiles = h->tma_tiles;
+	a.flag = h->flag;
 	return a;
 }
 
@@ -507,6 +560,7 @@ template <typename T> int do_steps(pfcg_handle* h, int nsteps) {
 	}
 	CK(h, cudaMemcpyAsync(h->h_flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
 	CK(h, cudaStreamSynchronize(h->stream));
+	if (*h->h_flag & FLAG_TIMEOUT) return fail(h, PFCG_ETIMEOUT, "a bounded device-side wait ran out (y-pass TMA load)");
 	if (*h->h_flag) return fail(h, PFCG_NAN, "Not a number value detected.");
 	return 0;
 }
@@ -824,6 +878,7 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	if (!rc && h->cys.spec)
 		rc = fp64 ? upload_ct_twiddles<double>(h, Ny, ct_radix(true, Ny), &h->twcty)
 		          : upload_ct_twiddles<float>(h, Ny, ct_radix(false, Ny), &h->twcty);
+	if (!rc) rc = setup_tma(h);
 	if (rc) return bail(rc);
 	*out = h;
 	return 0;
@@ -839,6 +894,7 @@ void pfcg_destroy(pfcg_handle* h) {
 	cudaFree(h->twy);
 	cudaFree(h->twctx);
 	cudaFree(h->twcty);
+	cudaFree(h->tmap);
 	cudaFree(h->mean);
 	cudaFree(h->acc);
 	cudaFree(h->offs);
@@ -1235,6 +1291,8 @@ template <typename T> void batch_args(pfcg_batch* b, std::vector<XArgs<T>>& xa, 
 		xa[i].acc = h->acc + ACC_NL;
 		xa[i].flag = b->d_flags + i;
 		ya[i] = yargs<T>(h);
+		ya[i].tmap = nullptr; // the batched y-pass keeps the plain loads
+		ya[i].flag = b->d_flags + i;
 	}
 }
 

@@ -113,7 +113,18 @@ template <typename T> struct YArgs {
 	int wkind, wsrc;        // YP_WEIGHT: weight kind and source field
 	WParams wp;             // YP_WEIGHT: parameters of the weight
 	int regio;              // STEP, specialised kernels: first/last transform pass to/from global memory
+	// STEP with register ends: a CUtensorMap (device memory) over `work` viewed as
+	// [field][tile][kx][row] with boxes (R rows, CC columns, tma_tiles tiles, 1
+	// field), through which the forward transform's input columns arrive by TMA;
+	// nullptr = plain loads. tma_tiles divides Ny / R.
+	const void* tmap;
+	int tma_tiles;
+	int* flag;              // bit 1: a bounded device wait ran out (PFCG_ETIMEOUT)
 };
+
+// Flag bits of the step kernels' status word
+constexpr int FLAG_NAN = 1;
+constexpr int FLAG_TIMEOUT = 2;
 
 struct LaunchCfg {
 	int grid, block, smem;
@@ -130,6 +141,8 @@ int spec_y_threads(bool fp64, int U, int N, bool fused);
 int spec_x_smem(bool fp64, int U, int N);
 int spec_y_smem(bool fp64, int U, int N);
 int spec_twiddles(bool fp64, int N);
+// 1 if that y-pass reads its input columns straight from memory (TMA-capable)
+int spec_y_regio(bool fp64, int U, int N);
 
 // Host-side launchers; return cudaGetLastError().
 template <typename T> cudaError_t launch_xpass(int mode, const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s);

@@ -31,6 +31,38 @@ template <typename T> static int ct_twn(int N) {
 }
 int spec_twiddles(bool fp64, int N) { return fp64 ? ct_twn<double>(N) : ct_twn<float>(N); }
 
+// whether the specialised y-pass (not the register-fused variant) of this
+// shape takes its first transform's input straight from memory (register
+// ends, the path that can load by TMA)
+template <typename T, int U, int N> static bool y_regio() {
+	constexpr int CC = Spec<T>::ycc(U, N), R = Spec<T>::xr(U, N);
+	using C = YCfg<T, U, N, CC, R, false>;
+	constexpr int M = C::MAXE;
+	return C::NSUB == C::S && C::S * (N / M) == C::NT && CtPlan<N, M>::FUSABLE;
+}
+template <typename T, int U> static bool y_regio_n(int N) {
+	switch (N) {
+	case 4096: return y_regio<T, U, 4096>();
+	case 2048: return y_regio<T, U, 2048>();
+	}
+	if constexpr (sizeof(T) == 4) {
+		switch (N) {
+		case 1536: return y_regio<T, U, 1536>();
+		case 1024: return y_regio<T, U, 1024>();
+		case 768: return y_regio<T, U, 768>();
+		case 512: return y_regio<T, U, 512>();
+		case 384: return y_regio<T, U, 384>();
+		case 256: return y_regio<T, U, 256>();
+		}
+	}
+	return false;
+}
+int spec_y_regio(bool fp64, int U, int N) {
+	if (U == 1) return fp64 ? y_regio_n<double, 1>(N) : y_regio_n<float, 1>(N);
+	if (U == 2) return fp64 ? y_regio_n<double, 2>(N) : y_regio_n<float, 2>(N);
+	return 0;
+}
+
 int spec_x_threads(bool fp64, int U, int N) {
 	const int maxe = ct_radix(fp64, N);
 	const int P = (U * spec_rows(fp64, U, N) + 1) / 2;

@@ -591,7 +591,7 @@ template <typename T, int U, int MODE, int NC, int RC>
 __device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile, const bool load_tw = true) {
 	using C = XCfg<T, U, NC, RC>;
 	constexpr int MAXE = C::MAXE;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
+	extern __shared__ __align__(128) unsigned char smem_raw[];
 	cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
 	const int Nx = C::CT ? NC : a.g.Nx;
 	const int Ny = a.g.Ny;
@@ -800,11 +800,55 @@ __global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MI
 
 // Body of the y-pass for column group `grp`; called by ypass_kernel and by
 // ypass_batch_kernel.
+// ------------------------------------------------------ TMA column loads --
+// The y-pass's input columns are R-row pieces of every row tile of `work`
+// (16 bytes per tile and column at 4096^2 U=2 FP32), a gather that costs the
+// load/store unit one request per 16 bytes. The tensor memory accelerator
+// moves them instead: thread 0 issues one cp.async.bulk.tensor per box of
+// tma_tiles tiles and field, the boxes land in shared memory as
+// [field][tile][column][row] (so field u, column c, row y of a column group
+// is at u * Ny * CC + ((y / R) * CC + c) * R + y % R), and the CTA waits on an
+// mbarrier. The wait is bounded: after about a second of polling it records
+// FLAG_TIMEOUT and goes on, and the step returns PFCG_ETIMEOUT. The tensor map
+// covers only this GPU's own `work` buffer and no load uses multicast.
+
+__device__ __forceinline__ void tma_bar_init(unsigned bar) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_expect(unsigned bar, unsigned bytes) {
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load4(unsigned dst, const void* tmap, int c0, int c1, int c2, int c3, unsigned bar) {
+	asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+	             "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+	             : "memory");
+}
+
+// polls phase `parity` of the mbarrier for at most ~1 s (%globaltimer); false on time-out
+__device__ __forceinline__ bool tma_wait(unsigned bar, unsigned parity) {
+	unsigned long long t0;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+	for (;;) {
+		unsigned done;
+		asm volatile("{ .reg .pred q; mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2; selp.u32 %0, 1, 0, q; }"
+		             : "=r"(done)
+		             : "r"(bar), "r"(parity)
+		             : "memory");
+		if (done) return true;
+		unsigned long long t;
+		asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+		if (t - t0 > 1000000000ull) return false;
+	}
+}
+
 template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
-__device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, const bool load_tw = true) {
+__device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, const bool load_tw = true, const int iter = 0) {
 	using C = YCfg<T, U, NC, CCC, RC, FUSEDK>;
 	constexpr int MAXE = C::MAXE;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
+	extern __shared__ __align__(128) unsigned char smem_raw[];
 	cplx<T>* sm = reinterpret_cast<cplx<T>*>(smem_raw);
 	const int Nx = a.g.Nx, H = a.g.H;
 	const int Ny = C::CT ? NC : a.g.Ny;
@@ -863,13 +907,43 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 		if (a.regio) {
 			regio = true;
 			RBY rb;
+			if (a.tmap) {
+				__shared__ __align__(8) unsigned long long tbar;
+				const unsigned bar = (unsigned)__cvta_generic_to_shared(&tbar);
+				if (iter == 0) {
+					if (tid == 0) tma_bar_init(bar);
+					__syncthreads();
+				}
+				constexpr int NTILE = NCX / RC;
+				if (tid == 0) {
+					const int tb = a.tma_tiles;
+					// earlier generic accesses to the buffer before the async-proxy writes
+					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+					tma_expect(bar, (unsigned)(U * NCX * CCX * sizeof(cplx<T>)));
+					for (int u = 0; u < U; u++)
+						for (int t0 = 0; t0 < NTILE; t0 += tb)
+							tma_load4((unsigned)__cvta_generic_to_shared(sm + (u * NTILE + t0) * CCX * RC), a.tmap, 0, kx0,
+							          t0, u, bar);
+				}
+				if (!tma_wait(bar, (unsigned)(iter & 1)) && tid == 0) atomicOr(a.flag, FLAG_TIMEOUT);
 #pragma unroll
-			for (int i = 0; i < RBY::NB; i++) {
-				const int p = RBY::seq(tid, i);
-				const bool live = p % CCX < ncol;
+				for (int i = 0; i < RBY::NB; i++) {
+					const int p = RBY::seq(tid, i);
 #pragma unroll
-				for (int r = 0; r < MAXE; r++)
-					rb.v[i][r] = live ? a.work[gaddr(p, RBY::pos(tid, i, r))] : mk<T>((T)0, (T)0);
+					for (int r = 0; r < MAXE; r++) {
+						const int y = RBY::pos(tid, i, r);
+						rb.v[i][r] = sm[((p / CCX) * NTILE + y / RC) * CCX * RC + (p % CCX) * RC + y % RC];
+					}
+				}
+			} else {
+#pragma unroll
+				for (int i = 0; i < RBY::NB; i++) {
+					const int p = RBY::seq(tid, i);
+					const bool live = p % CCX < ncol;
+#pragma unroll
+					for (int r = 0; r < MAXE; r++)
+						rb.v[i][r] = live ? a.work[gaddr(p, RBY::pos(tid, i, r))] : mk<T>((T)0, (T)0);
+				}
 			}
 			ct_first_from_regs<NCX, MAXE, C::S, C::NT, -1, T>(sm, rb, tid);
 			ct_middle<NCX, MAXE, C::S, C::NT, -1, T>(sm, tws, tid);
@@ -1201,7 +1275,7 @@ __global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC, FUSEDK>::NT, YCfg<T, U
 	// column groups blockIdx.x, + gridDim.x, ... (as the x-pass's tiles)
 	for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
 		if (g != (int)blockIdx.x) __syncthreads();
-		ypass_body<T, U, MODE, NC, CCC, RC, FUSEDK>(a, g, g == (int)blockIdx.x);
+		ypass_body<T, U, MODE, NC, CCC, RC, FUSEDK>(a, g, g == (int)blockIdx.x, (g - (int)blockIdx.x) / (int)gridDim.x);
 	}
 }
 

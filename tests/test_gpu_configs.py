@@ -114,4 +114,8 @@ def test_c3_heterostructure_4096_box_optimisation_10000_steps():
     print("C3 box-opt: rel d(box) fp32", box_f32.tolist(), "control", box_ctl.tolist())
     assert np.all(np.abs(b[:, 4:] - a[:, 4:]) < 1e-14)   # the means are conserved exactly
     assert a[-1, 3] < a[0, 3] and a[-1, 1] != a[0, 1]     # relaxed, and the box did move
-    assert rel_f32.max() < 1e-4 and box_f32.max() < 1e-4
+    # measured on B200: FP32 up to 1.4e-5 in <f> (at 500 steps, the ordering transient) and 6e-7 in
+    # the box; the FP64 control stays below 2e-13 and 6e-11, so FP32 rounding, not chaos, sets the gap
+    assert rel_f32.max() < 3e-5 and box_f32.max() < 2e-6
+    assert rel_f32[-1] < 1e-6                                # the relaxed end state meets the FP32 bound
+    assert rel_ctl.max() < 1e-11 and box_ctl.max() < 1e-9
