@@ -76,6 +76,11 @@ struct pfcg_handle {
 	int regio = 1;              // y-pass register ends (PFCG_YPASS_REGIO=0: load/store phases through shared memory)
 	void* tmap = nullptr;       // device copy of the y-pass's TMA tensor map over `work` (null: plain loads)
 	int tma_tiles = 0;          // row tiles per TMA box
+	// Test hook of the bounded wait (PFCG_TMA_TEST_STALL=<bytes> when the handle is created): the
+	// wait expects that many bytes more than the loads bring, so it runs out after 1 ms and the
+	// step reports PFCG_ETIMEOUT; no load or store changes.
+	unsigned tma_extra = 0;
+	unsigned long long tma_timeout_ns = 1000000000ull;
 	long long launches = 0;
 	// per-kernel timing (pfcg_set_profiling)
 	bool profiling = false;
@@ -345,6 +350,11 @@ int setup_tma(pfcg_handle* h) {
 	CK(h, cudaMalloc(&h->tmap, sizeof(CUtensorMap)));
 	CK(h, cudaMemcpy(h->tmap, &tm, sizeof(CUtensorMap), cudaMemcpyHostToDevice));
 	h->tma_tiles = tb;
+	const char* stall = std::getenv("PFCG_TMA_TEST_STALL");
+	if (stall && std::atoi(stall) > 0) {
+		h->tma_extra = (unsigned)std::atoi(stall) & ~15u;
+		h->tma_timeout_ns = 1000000ull;
+	}
 	return 0;
 }
 
@@ -428,6 +438,8 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.regio = h->regio;
 	a.tmap = h->tmap;
 	a.tma_tiles = h->tma_tiles;
+	a.tma_extra = h->tma_extra;
+	a.tma_timeout_ns = h->tma_timeout_ns;
 	a.flag = h->flag;
 	return a;
 }

@@ -119,6 +119,8 @@ template <typename T> struct YArgs {
 	// nullptr = plain loads. tma_tiles divides Ny / R.
 	const void* tmap;
 	int tma_tiles;
+	unsigned tma_extra;     // bytes the wait expects beyond the loads (0; > 0 only to test the time-out)
+	unsigned long long tma_timeout_ns; // bound of that wait
 	int* flag;              // bit 1: a bounded device wait ran out (PFCG_ETIMEOUT)
 };
 

@@ -808,8 +808,8 @@ __global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MI
 // tma_tiles tiles and field, the boxes land in shared memory as
 // [field][tile][column][row] (so field u, column c, row y of a column group
 // is at u * Ny * CC + ((y / R) * CC + c) * R + y % R), and the CTA waits on an
-// mbarrier. The wait is bounded: after about a second of polling it records
-// FLAG_TIMEOUT and goes on, and the step returns PFCG_ETIMEOUT. The tensor map
+// mbarrier. The wait is bounded: after tma_timeout_ns (1 s) of polling it
+// records FLAG_TIMEOUT and goes on, and the step returns PFCG_ETIMEOUT. The tensor map
 // covers only this GPU's own `work` buffer and no load uses multicast.
 
 __device__ __forceinline__ void tma_bar_init(unsigned bar) {
@@ -827,8 +827,8 @@ __device__ __forceinline__ void tma_load4(unsigned dst, const void* tmap, int c0
 	             : "memory");
 }
 
-// polls phase `parity` of the mbarrier for at most ~1 s (%globaltimer); false on time-out
-__device__ __forceinline__ bool tma_wait(unsigned bar, unsigned parity) {
+// polls phase `parity` of the mbarrier for at most `limit_ns` (%globaltimer); false on time-out
+__device__ __forceinline__ bool tma_wait(unsigned bar, unsigned parity, unsigned long long limit_ns) {
 	unsigned long long t0;
 	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
 	for (;;) {
@@ -840,7 +840,7 @@ __device__ __forceinline__ bool tma_wait(unsigned bar, unsigned parity) {
 		if (done) return true;
 		unsigned long long t;
 		asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-		if (t - t0 > 1000000000ull) return false;
+		if (t - t0 > limit_ns) return false;
 	}
 }
 
@@ -919,13 +919,13 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 					const int tb = a.tma_tiles;
 					// earlier generic accesses to the buffer before the async-proxy writes
 					asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-					tma_expect(bar, (unsigned)(U * NCX * CCX * sizeof(cplx<T>)));
+					tma_expect(bar, (unsigned)(U * NCX * CCX * sizeof(cplx<T>)) + a.tma_extra);
 					for (int u = 0; u < U; u++)
 						for (int t0 = 0; t0 < NTILE; t0 += tb)
 							tma_load4((unsigned)__cvta_generic_to_shared(sm + (u * NTILE + t0) * CCX * RC), a.tmap, 0, kx0,
 							          t0, u, bar);
 				}
-				if (!tma_wait(bar, (unsigned)(iter & 1)) && tid == 0) atomicOr(a.flag, FLAG_TIMEOUT);
+				if (!tma_wait(bar, (unsigned)(iter & 1), a.tma_timeout_ns) && tid == 0) atomicOr(a.flag, FLAG_TIMEOUT);
 #pragma unroll
 				for (int i = 0; i < RBY::NB; i++) {
 					const int p = RBY::seq(tid, i);
