@@ -1303,8 +1303,7 @@ template <typename T> void batch_args(pfcg_batch* b, std::vector<XArgs<T>>& xa, 
 		xa[i].acc = h->acc + ACC_NL;
 		xa[i].flag = b->d_flags + i;
 		ya[i] = yargs<T>(h);
-		ya[i].tmap = nullptr; // the batched y-pass keeps the plain loads
-		ya[i].flag = b->d_flags + i;
+		ya[i].flag = b->d_flags + i; // NaN and wait time-out of problem i
 	}
 }
 
@@ -1539,6 +1538,11 @@ int pfcg_batch_step(pfcg_batch* b, int nsteps) {
 		h->t += nsteps;
 		h->launches += 2 * nsteps;
 	}
+	for (int i = 0; i < n; i++)
+		if (b->h_flags[i] & FLAG_TIMEOUT) {
+			g_err = "a bounded device-side wait ran out (y-pass TMA load)";
+			return PFCG_ETIMEOUT;
+		}
 	for (int i = 0; i < n; i++)
 		if (b->h_flags[i]) { g_err = "Not a number value detected."; return PFCG_NAN; }
 	return 0;
