@@ -451,6 +451,35 @@ def ttr_arms(N: int, max_steps: int, Topt: int = 100) -> dict:
     return arms
 
 
+def run_fno_train(B: int, iters: int):
+    """One training iteration of the warm-start network (loss and gradients,
+    then an Adam step) on B random 512^2 two-field tiles, after two untimed
+    iterations; CUDA-synchronised wall time."""
+    import torch
+
+    from pfc_b200 import fno
+
+    with fno.Network(512, B) as net:
+        net.set_params(fno.init_params(0))
+        g = torch.Generator(device="cuda").manual_seed(0)
+        x = torch.randn((B, 2, 512, 512), device="cuda", dtype=torch.float32, generator=g) * 0.3
+        t = x + 0.01 * torch.randn(x.shape, device="cuda", dtype=torch.float32, generator=g)
+        torch.cuda.synchronize()
+        for _ in range(2):
+            net.loss_grad(x.data_ptr(), t.data_ptr(), B)
+            net.adam_step(1e-4)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(iters):
+            net.loss_grad(x.data_ptr(), t.data_ptr(), B)
+            net.adam_step(1e-4)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / iters
+    print(json.dumps({"metric": "warm-start network training iteration (512^2 tiles)", "value": dt * 1e3,
+                      "unit": "ms", "higher_is_better": False, "tiles": B, "iters": iters,
+                      "ms_per_tile": dt * 1e3 / B, "data": "synthetic"}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -474,6 +503,9 @@ def main():
     ap.add_argument("--ttr-topt", type=int, default=100, help="box optimisation period of the time-to-relaxed arms")
     ap.add_argument("--ttr-reps", type=int, default=1, help="repeats of the time-to-relaxed arms (median reported)")
     ap.add_argument("--no-ttr", action="store_true", help="leave the time-to-relaxed arms out of the default line")
+    ap.add_argument("--fno-train", type=int, default=0, metavar="B",
+                    help="time one warm-start network training iteration on B tiles of 512^2 instead")
+    ap.add_argument("--fno-iters", type=int, default=10)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -485,6 +517,10 @@ def main():
     if args.batch:
         lib.set_device(local)
         run_batch(args)
+        return
+    if args.fno_train:
+        lib.set_device(local)
+        run_fno_train(args.fno_train, args.fno_iters)
         return
     if args.ttr:
         if rank == 0:

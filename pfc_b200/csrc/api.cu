@@ -441,6 +441,7 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.tma_extra = h->tma_extra;
 	a.tma_timeout_ns = h->tma_timeout_ns;
 	a.flag = h->flag;
+	a.k = host_step_k<T>(h->model, h->geom);
 	return a;
 }
 

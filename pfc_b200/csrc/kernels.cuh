@@ -69,6 +69,21 @@ enum YMode { YP_STEP = 0, YP_INIT = 1, YP_WEIGHT = 2 };
 // (W_OR) and a Gaussian-smoothed derivative (W_DG)
 enum WKind { W_ONE = 0, W_P = 1, W_G = 2, W_Q = 3, W_GS = 4, W_OR = 5, W_DG = 6 };
 
+// Model constants of the y-pass update in the transform precision, filled on
+// the host (host_step_k): as kernel parameters the instructions that use them
+// read them straight from the constant bank, with no conversion and no
+// register held across the update.
+template <typename T> struct StepK {
+	T invN, cc, dt, ag;
+	int semi;
+	int W[MAXU];
+	T alpha[MAXU], betad[MAXU];
+	T nu2[MAXU][MAXW], omega[MAXU][MAXW], phi[MAXU][MAXW];
+	T beta[MAXU][MAXU], eps[MAXU][MAXU], mu2[MAXU][MAXU];
+	T dkx, dky;
+};
+template <typename T> StepK<T> host_step_k(const Model& m, const Geom& g);
+
 template <typename T> struct XArgs {
 	cplx<T>* work;          // U arrays at stride wstride
 	long long wstride;
@@ -122,6 +137,7 @@ template <typename T> struct YArgs {
 	unsigned tma_extra;     // bytes the wait expects beyond the loads (0; > 0 only to test the time-out)
 	unsigned long long tma_timeout_ns; // bound of that wait
 	int* flag;              // bit 1: a bounded device wait ran out (PFCG_ETIMEOUT)
+	StepK<T> k;             // STEP: the update's constants
 };
 
 // Flag bits of the step kernels' status word

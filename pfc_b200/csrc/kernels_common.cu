@@ -239,3 +239,37 @@ cudaError_t launch_scaled_acc(double* acc, const double* r, long long n, double*
 }
 
 } // namespace pfcg
+
+namespace pfcg {
+
+template <typename T> StepK<T> host_step_k(const Model& m, const Geom& g) {
+	StepK<T> k{};
+	k.invN = (T)(1.0 / ((double)g.Nx * (double)g.Ny));
+	k.cc = (T)m.c;
+	k.dt = (T)m.dt;
+	k.ag = (T)(-0.5 / m.sigma / m.sigma);
+	k.semi = m.scheme == SCHEME_SEMI;
+	for (int u = 0; u < MAXU; u++) {
+		k.W[u] = m.W[u];
+		k.alpha[u] = (T)m.alpha[u][u];
+		k.betad[u] = (T)m.beta[u][u];
+		for (int w = 0; w < MAXW; w++) {
+			k.nu2[u][w] = (T)m.nu2[u][w];
+			k.omega[u][w] = (T)m.omega[u][w];
+			k.phi[u][w] = (T)m.phi[u][w];
+		}
+		for (int v = 0; v < MAXU; v++) {
+			k.beta[u][v] = (T)m.beta[u][v];
+			k.eps[u][v] = (T)m.epsilon[u][v];
+			k.mu2[u][v] = (T)m.mu2[u][v];
+		}
+	}
+	k.dkx = (T)g.dkx;
+	k.dky = (T)g.dky;
+	return k;
+}
+
+template StepK<float> host_step_k<float>(const Model&, const Geom&);
+template StepK<double> host_step_k<double>(const Model&, const Geom&);
+
+} // namespace pfcg

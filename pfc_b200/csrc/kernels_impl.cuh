@@ -109,7 +109,10 @@ template <typename T> __device__ __forceinline__ T k2_step(int kx, int ky, int N
 // phi1(x) = (exp(x) - 1) / x given A = exp(x): Taylor series to x^6 / 7! for
 // |x| < 1/4 (remainder < 2e-9), the quotient otherwise (relative error below
 // 3e-7 in FP32). B = (A - 1)/a = o dt phi1(x) with x = o a dt, which is also
-// the reference's a = 0 case (pfc-relax.c:951-952).
+// the reference's a = 0 case (pfc-relax.c:951-952). The quotient is the
+// correctly rounded division: __fdividef (2 ulp) was 0.4 % faster per step but
+// moved the relaxed 4096^2 heterostructure's FP32 energy from 1.6e-7 to 2.6e-6
+// of the FP64 one (the box optimisation picked other trial sizes).
 __device__ __forceinline__ float phi1f(float x, float A) {
 	if (fabsf(x) < 0.25f)
 		return 1.f + x * (0.5f + x * (1.f / 6.f + x * (1.f / 24.f + x * (1.f / 120.f + x * (1.f / 720.f + x * (1.f / 5040.f))))));
@@ -143,49 +146,13 @@ template <typename T, int U, int NC, int CCC, int RC, bool FUSEDK = true> struct
 	static constexpr int TWN = CT ? CtPlan<NC, MAXE>::TWN : 0;
 };
 
-// Model constants of the k-space update converted once to the transform
-// precision (converting inside the per-entry loop costs an F2F per use).
-template <typename T, int U> struct StepConsts {
-	T invN, cc, dt, ag;
-	bool semi; // SCHEME_SEMI
-	int W[U];
-	T alpha[U], betad[U];
-	T nu2[U][MAXW], omega[U][MAXW], phi[U][MAXW];
-	T beta[U][U], eps[U][U], mu2[U][U];
-	__device__ __forceinline__ StepConsts(const Model& m, int Nx, int Ny) {
-		invN = (T)(1.0 / ((double)Nx * (double)Ny));
-		cc = (T)m.c;
-		dt = (T)m.dt;
-		ag = (T)(-0.5 / m.sigma / m.sigma);
-		semi = m.scheme == SCHEME_SEMI;
-#pragma unroll
-		for (int u = 0; u < U; u++) {
-			W[u] = m.W[u];
-			alpha[u] = (T)m.alpha[u][u];
-			betad[u] = (T)m.beta[u][u];
-#pragma unroll
-			for (int w = 0; w < MAXW; w++) {
-				nu2[u][w] = (T)m.nu2[u][w];
-				omega[u][w] = (T)m.omega[u][w];
-				phi[u][w] = (T)m.phi[u][w];
-			}
-#pragma unroll
-			for (int v = 0; v < U; v++) {
-				beta[u][v] = (T)m.beta[u][v];
-				eps[u][v] = (T)m.epsilon[u][v];
-				mu2[u][v] = (T)m.mu2[u][v];
-			}
-		}
-	}
-};
-
 // ETD coefficients of one (kx, ky) entry (pfc-relax.c:940-955 and the coupling
 // terms of :1215-1244): A_u = exp(o a_u dt) and B_u (FP32: o dt phi1(o a_u dt);
 // FP64: the reference's (A - 1)/a, o dt at a = 0) for every field, and the
 // coupling coefficient beta_uv (mu2_uv - k2)^2 + eps_uv G^2 of every pair u < v.
 template <typename T, int U> __host__ __device__ constexpr int npairs() { return U * (U - 1) / 2 > 0 ? U * (U - 1) / 2 : 1; }
 template <typename T, int U>
-__device__ __forceinline__ void entry_coef(const StepConsts<T, U>& K, T k2, T (&A)[U], T (&Bn)[U],
+__device__ __forceinline__ void entry_coef(const StepK<T>& K, T k2, T (&A)[U], T (&Bn)[U],
                                            T (&cu)[npairs<T, U>()]) {
 	if constexpr (U > 1) {
 		const T G = expT<T>(K.ag * k2);
@@ -268,7 +235,7 @@ __device__ __forceinline__ void hermitian_column(cplx<T>* col, cplx<T>* spec_col
 // the first pass of the next (fft_core.cuh, RegBlock), so the pointwise work
 // between two transforms costs no shared-memory round trip and no barrier.
 
-template <typename T, int U> __device__ __forceinline__ T pick(const T (&a)[U], int u) {
+template <typename T, int U, int N> __device__ __forceinline__ T pick(const T (&a)[N], int u) {
 	T r = a[0];
 #pragma unroll
 	for (int k = 1; k < U; k++)
@@ -490,8 +457,8 @@ __device__ __forceinline__ void ypass_step_fused(const YArgs<T>& a, cplx<T>* sm,
 
 	// update, pfc-relax.c:1215-1244 (A, B of update_AB, :901-958, recomputed);
 	// the field's own constants, selected once
-	const StepConsts<T, U> K(a.m, Nx, NC);
-	const T dkxT = (T)a.g.dkx, dkyT = (T)a.g.dky;
+	const StepK<T>& K = a.k;
+	const T dkxT = K.dkx, dkyT = K.dky;
 	const T alpha = pick<T, U>(K.alpha, u), betad = pick<T, U>(K.betad, u);
 	const int W = pick<int, U>(K.W, u);
 	T nu2[MAXW], om[MAXW], ph[MAXW];
@@ -792,6 +759,10 @@ __device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile, co
 template <typename T, int U, int MODE, int NC, int RC>
 __global__ void __launch_bounds__(XCfg<T, U, NC, RC>::NT, XCfg<T, U, NC, RC>::MINB)
     xpass_kernel(const XArgs<T> a, int ntiles) {
+	// programmatic dependent launch (pdl_launch): the previous kernel's results
+	// are complete and visible after this wait; a plain launch returns at once
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	asm volatile("griddepcontrol.launch_dependents;");
 	for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
 		if (t != (int)blockIdx.x) __syncthreads(); // the previous tile's readers of shared memory are done
 		xpass_body<T, U, MODE, NC, RC>(a, t, t == (int)blockIdx.x);
@@ -997,8 +968,8 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 	const double dx = a.g.dx, dy = a.g.dy;
 	if constexpr (MODE == YP_STEP) {
 		// model constants in the transform precision, once per CTA
-		const StepConsts<T, U> K(a.m, Nx, Ny);
-		const T dkxT = (T)a.g.dkx, dkyT = (T)a.g.dky;
+		const StepK<T>& K = a.k;
+		const T dkxT = K.dkx, dkyT = K.dky;
 		// update of one (kx, ky) entry for all fields with its coefficients
 		// (A, B, couplings of k^2), pfc-relax.c:1215-1244
 		auto apply = [&](int c, int kx, int ky, const cplx<T>(&Nv)[U], const T(&A)[U], const T(&Bn)[U],
@@ -1272,6 +1243,8 @@ __global__ void __launch_bounds__(256) kspace_energy_kernel(const cplx<T>* __res
 template <typename T, int U, int MODE, int NC, int CCC, int RC, bool FUSEDK = true>
 __global__ void __launch_bounds__(YCfg<T, U, NC, CCC, RC, FUSEDK>::NT, YCfg<T, U, NC, CCC, RC, FUSEDK>::MINB)
     ypass_kernel(const YArgs<T> a, int ngroups) {
+	asm volatile("griddepcontrol.wait;" ::: "memory"); // as in xpass_kernel
+	asm volatile("griddepcontrol.launch_dependents;");
 	// column groups blockIdx.x, + gridDim.x, ... (as the x-pass's tiles)
 	for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
 		if (g != (int)blockIdx.x) __syncthreads();
@@ -1362,6 +1335,38 @@ template <typename K> static int resident_grid(K k, const LaunchCfg& c, int& res
 	return resident > 0 && resident < c.grid ? resident : c.grid;
 }
 
+// Launch of the x- and y-pass kernels as programmatic dependent launches: the
+// next pass's CTAs may be scheduled while the last wave of the previous one
+// drains, and each kernel waits for the previous kernel's completion and
+// memory (griddepcontrol.wait, its first statement) before touching anything
+// that kernel writes. PFCG_PDL=0 launches them plainly.
+static bool pdl_on() {
+	static const int on = [] {
+		const char* e = std::getenv("PFCG_PDL");
+		return (e && e[0] == '0') ? 0 : 1;
+	}();
+	return on != 0;
+}
+
+template <typename K, typename A>
+static cudaError_t pdl_launch(K k, int grid, int block, int smem, cudaStream_t s, const A& a, int n) {
+	if (!pdl_on()) {
+		k<<<grid, block, smem, s>>>(a, n);
+		return cudaGetLastError();
+	}
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(grid);
+	cfg.blockDim = dim3(block);
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = s;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	at[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, k, a, n);
+}
+
 template <typename T, int U, int MODE, int NC, int RC>
 static cudaError_t xlaunch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s) {
 	auto k = xpass_kernel<T, U, MODE, NC, RC>;
@@ -1369,8 +1374,7 @@ static cudaError_t xlaunch(const XArgs<T>& a, const LaunchCfg& c, cudaStream_t s
 	static int resident = 0;
 	smem_attr(k, mask);
 	const int grid = NC > 0 && std::is_same<T, double>::value ? resident_grid(k, c, resident) : c.grid;
-	k<<<grid, c.block, c.smem, s>>>(a, c.grid);
-	return cudaGetLastError();
+	return pdl_launch(k, grid, c.block, c.smem, s, a, c.grid);
 }
 
 // Compile-time specialisations of the STEP kernels: (length, rows per tile,
@@ -1383,8 +1387,7 @@ static cudaError_t ylaunch(const YArgs<T>& a, const LaunchCfg& c, cudaStream_t s
 	static int resident = 0;
 	smem_attr(k, mask);
 	const int grid = NC > 0 && std::is_same<T, double>::value ? resident_grid(k, c, resident) : c.grid;
-	k<<<grid, c.block, c.smem, s>>>(a, c.grid);
-	return cudaGetLastError();
+	return pdl_launch(k, grid, c.block, c.smem, s, a, c.grid);
 }
 
 template <typename T> struct Spec;
