@@ -6,11 +6,12 @@
 //   y = x + Q v_L + q                       projection C -> 2, added to the input
 // K_l v = irfft2 of R_l (complex C x C per retained mode) times rfft2(v) on the
 // retained modes kx in [0, MX), ky in {0..MY/2-1} u {T-MY/2..T-1}; all other
-// modes are dropped. The truncated transforms are direct sums against a
-// twiddle table (dft_x, dft_y, idft_x); the adjoint of each linear step is
-// another of these kernels, which is how the backward pass is built:
-//   idft_x^T = dft_x with the inverse's per-mode weights, dft_y^T = the
-//   inverse y sum, mix^T = mix with conj(R) transposed, dft_x^T = idft_x.
+// modes are dropped. The truncated transforms are direct sums against
+// twiddle matrices (dft_x, idft_x, dft_y_fwd, dft_y_inv); the adjoint of each
+// linear step is another of these kernels, which is how the backward pass is
+// built:
+//   idft_x^T = dft_x with the inverse's per-mode weights, dft_y_fwd^T =
+//   dft_y_inv, mix^T = mix with conj(R) transposed, dft_x^T = idft_x.
 // Activations and sums are FP32; the kernels read a BF16 copy of the FP32
 // master weights, which Adam updates.
 #include <cuda_bf16.h>
@@ -60,11 +61,6 @@ __device__ __forceinline__ float gelu_d(float z) {
 
 // wave number of retained row k along y
 __device__ __forceinline__ int ky_of(int k, int T) { return k < MY / 2 ? k : T - MY + k; }
-
-__device__ __forceinline__ void load_tw(float2* sh, const float2* __restrict__ tw, int T) {
-	for (int i = threadIdx.x; i < T; i += blockDim.x) sh[i] = tw[i];
-	__syncthreads();
-}
 
 template <typename A> __device__ __forceinline__ A warp_sum(A a) {
 	for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -258,59 +254,204 @@ __global__ void __launch_bounds__(256) idft_x(const float2* __restrict__ in, flo
 	}
 }
 
-// Along y for each plane of [rows][MX] complex values:
+// The truncated transforms along y, per plane of [rows][MX] complex values:
 //   forward: out[k][m] = sum_y in[y][m] exp(-2 pi i ky(k) y / T), k < MY
 //   inverse: out[y][m] = sum_k in[k][m] exp(+2 pi i ky(k) y / T), y < T
-__global__ void dft_y(const float2* __restrict__ in, float2* __restrict__ out, const float2* __restrict__ tw,
-                      long long nplanes, int T, int inverse) {
-	__shared__ float2 sh[MAXT];
-	load_tw(sh, tw, T);
-	const int nout = inverse ? T : MY;
-	const int nin = inverse ? MY : T;
+// are GEMMs against fixed twiddle matrices, on the tensor cores with one warp
+// per plane. The twiddles are the A operand, their BF16-split fragments
+// tabulated once per tile size (dfty_frag_kernel); the plane's values are the
+// B operand, split per use, with three products (hi hi, hi lo, lo hi):
+//   forward: D[k][2m + q] = sum_{y, c} E[k][2y + c] Z[2y + c][2m + q], (E[k][2y], E[k][2y + 1]) = (cos, sin)(2 pi ky(k) y / T)
+//   inverse: D[y][2m + q] = sum_{k, c} F[y][2k + c] Z[2k + c][2m + q], (F[y][2k], F[y][2k + 1]) = (cos, -sin)(2 pi ky(k) y / T)
+// with Z[2j][2m] = Re z[j][m], Z[2j + 1][2m] = Im, Z[2j][2m + 1] = Im, Z[2j + 1][2m + 1] = -Re, so that
+// the accumulator pair of columns 2t, 2t + 1 is one output's (Re, Im).
+static_assert(MY == 16 && MX == 8, "one m16 tile of modes and two n8 tiles of (Re, Im) columns");
+
+// fdy: [T/8 k-steps][32 lanes][hi, lo], fiy: [T/16 m-tiles][2 k-steps][32 lanes][hi, lo];
+// each uint4 holds the four A registers (rows g, g + 8 by columns 2t, 2t + 8)
+__global__ void dfty_frag_kernel(const float2* __restrict__ tw, int T, uint4* __restrict__ fdy, uint4* __restrict__ fiy) {
+	const int nf = T / 8 * 32, ni = T / 16 * 2 * 32;
+	for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nf + ni; e += gridDim.x * blockDim.x) {
+		const bool fwd = e < nf;
+		const int f = fwd ? e : e - nf;
+		const int lane = f & 31, g = lane >> 2, t = lane & 3;
+		int rows[2], cols[2];
+		if (fwd) {
+			const int ks = f >> 5;
+			rows[0] = g;
+			rows[1] = g + 8;
+			cols[0] = 8 * ks + t;
+			cols[1] = cols[0] + 4;
+		} else {
+			const int ks = (f >> 5) & 1, mt = f >> 6;
+			rows[0] = 16 * mt + g;
+			rows[1] = rows[0] + 8;
+			cols[0] = 8 * ks + t;
+			cols[1] = cols[0] + 4;
+		}
+		uint32_t hi[4], lo[4];
+#pragma unroll
+		for (int r = 0; r < 4; r++) {
+			// register r: row rows[r & 1], column pair of cols[r >> 1]
+			const int row = rows[r & 1], col = cols[r >> 1];
+			const int ky = ky_of(fwd ? row : col, T), y = fwd ? col : row;
+			const float2 w = tw[(ky * y) & (T - 1)];
+			split2(w.x, fwd ? w.y : -w.y, hi[r], lo[r]);
+		}
+		uint4* dst = (fwd ? fdy : fiy) + 2 * f;
+		dst[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+		dst[1] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+	}
+}
+
+// the B registers of value z in the output column of parity q: (Re, Im) or (Im, -Re)
+__device__ __forceinline__ void zsplit(float2 z, int q, uint32_t& hi, uint32_t& lo) {
+	if (q) split2(z.y, -z.x, hi, lo);
+	else split2(z.x, z.y, hi, lo);
+}
+
+// One block of four warps per plane. Forward: warp w takes the k-steps
+// w, w + 4, ... and the warps' partial sums are added in shared memory in a
+// fixed order. Inverse: warp w takes the m-tiles w, w + 4, ...
+constexpr int DY_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * DY_WARPS) dft_y_fwd(const float2* __restrict__ in, float2* __restrict__ out,
+                                                          const uint4* __restrict__ fdy, long long nplanes, int T) {
+	__shared__ float red[DY_WARPS][32][8];
+	const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3, q = g & 1;
 	for (long long plane = blockIdx.x; plane < nplanes; plane += gridDim.x) {
-		const float2* pin = in + plane * nin * MX;
-		float2* pout = out + plane * nout * MX;
-		for (int o = threadIdx.x; o < nout * MX; o += blockDim.x) {
-			const int q = o / MX, m = o - q * MX;
-			float ar = 0.f, ai = 0.f;
-			for (int j = 0; j < nin; j++) {
-				const int y = inverse ? q : j;
-				const int ky = ky_of(inverse ? j : q, T);
-				const float2 e = sh[(ky * y) & (T - 1)];
-				const float s = inverse ? e.y : -e.y;
-				const float2 z = pin[j * MX + m];
-				ar += z.x * e.x - z.y * s;
-				ai += z.x * s + z.y * e.x;
+		const float2* pin = in + plane * T * MX;
+		float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+		for (int ks = wp; ks < T / 8; ks += DY_WARPS) {
+			const uint4 fh = __ldg(fdy + (ks * 32 + lane) * 2), fl = __ldg(fdy + (ks * 32 + lane) * 2 + 1);
+			const uint32_t ah[4] = {fh.x, fh.y, fh.z, fh.w}, al[4] = {fl.x, fl.y, fl.z, fl.w};
+			const int y0 = 8 * ks + t;
+#pragma unroll
+			for (int nt = 0; nt < 2; nt++) {
+				const int m = 4 * nt + (g >> 1);
+				uint32_t bh[2], bl[2];
+				zsplit(pin[y0 * MX + m], q, bh[0], bl[0]);
+				zsplit(pin[(y0 + 4) * MX + m], q, bh[1], bl[1]);
+				mma_bf16(d[nt], ah, bh);
+				mma_bf16(d[nt], ah, bl);
+				mma_bf16(d[nt], al, bh);
 			}
-			pout[o] = make_float2(ar, ai);
+		}
+		__syncthreads(); // the previous plane's sums have been read
+#pragma unroll
+		for (int j = 0; j < 8; j++) red[wp][lane][j] = d[j >> 2][j & 3];
+		__syncthreads();
+		if (wp == 0) {
+#pragma unroll
+			for (int j = 0; j < 8; j++) d[j >> 2][j & 3] = red[0][lane][j] + red[1][lane][j] + red[2][lane][j] + red[3][lane][j];
+			float2* pout = out + plane * MY * MX;
+#pragma unroll
+			for (int nt = 0; nt < 2; nt++) {
+				const int m = 4 * nt + t;
+				pout[g * MX + m] = make_float2(d[nt][0], d[nt][1]);
+				pout[(g + 8) * MX + m] = make_float2(d[nt][2], d[nt][3]);
+			}
 		}
 	}
 }
 
-// mode mixing, per retained mode km:
+__global__ void __launch_bounds__(32 * DY_WARPS) dft_y_inv(const float2* __restrict__ in, float2* __restrict__ out,
+                                                          const uint4* __restrict__ fiy, long long nplanes, int T) {
+	const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3, q = g & 1;
+	for (long long plane = blockIdx.x; plane < nplanes; plane += gridDim.x) {
+		const float2* pin = in + plane * MY * MX;
+		// the whole plane as B fragments: two k-steps (K = 2 MY) by two n-tiles
+		uint32_t bh[2][2][2], bl[2][2][2];
+#pragma unroll
+		for (int ks = 0; ks < 2; ks++)
+#pragma unroll
+			for (int nt = 0; nt < 2; nt++) {
+				const int k0 = 8 * ks + t, m = 4 * nt + (g >> 1);
+				zsplit(pin[k0 * MX + m], q, bh[ks][nt][0], bl[ks][nt][0]);
+				zsplit(pin[(k0 + 4) * MX + m], q, bh[ks][nt][1], bl[ks][nt][1]);
+			}
+		float2* pout = out + plane * T * MX;
+		for (int mt = wp; mt < T / 16; mt += DY_WARPS) {
+			float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+			for (int ks = 0; ks < 2; ks++) {
+				const uint4 fh = __ldg(fiy + ((mt * 2 + ks) * 32 + lane) * 2);
+				const uint4 fl = __ldg(fiy + ((mt * 2 + ks) * 32 + lane) * 2 + 1);
+				const uint32_t ah[4] = {fh.x, fh.y, fh.z, fh.w}, al[4] = {fl.x, fl.y, fl.z, fl.w};
+#pragma unroll
+				for (int nt = 0; nt < 2; nt++) {
+					mma_bf16(d[nt], ah, bh[ks][nt]);
+					mma_bf16(d[nt], ah, bl[ks][nt]);
+					mma_bf16(d[nt], al, bh[ks][nt]);
+				}
+			}
+			const int y0 = 16 * mt + g;
+#pragma unroll
+			for (int nt = 0; nt < 2; nt++) {
+				const int m = 4 * nt + t;
+				pout[y0 * MX + m] = make_float2(d[nt][0], d[nt][1]);
+				pout[(y0 + 8) * MX + m] = make_float2(d[nt][2], d[nt][3]);
+			}
+		}
+	}
+}
+
+// Mode mixing, per retained mode km:
 //   forward: out[b][o][km] = sum_i R[i][o][km] in[b][i][km]
 //   adjoint: out[b][i][km] = sum_o conj(R[i][o][km]) in[b][o][km]
-__global__ void mix(const float2* __restrict__ in, float2* __restrict__ out, const __nv_bfloat16* __restrict__ w, int l,
-                    int B, int adjoint) {
-	const long long n = (long long)B * C * NK;
-	const __nv_bfloat16* Rr = w + off_Rr(l);
-	const __nv_bfloat16* Ri = w + off_Ri(l);
-	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-		const int km = (int)(t % NK);
-		const int o = (int)((t / NK) % C);
-		const long long b = t / ((long long)NK * C);
-		const float2* ib = in + b * C * NK + km;
-		float ar = 0.f, ai = 0.f;
-#pragma unroll 8
-		for (int i = 0; i < C; i++) {
-			const size_t ri = adjoint ? ((size_t)o * C + i) * NK + km : ((size_t)i * C + o) * NK + km;
-			const float rr = __bfloat162float(Rr[ri]);
-			const float rm = adjoint ? -__bfloat162float(Ri[ri]) : __bfloat162float(Ri[ri]);
-			const float2 z = ib[(long long)i * NK];
-			ar += rr * z.x - rm * z.y;
-			ai += rr * z.y + rm * z.x;
+// On the tensor cores, one warp per mode and 16 batch rows: D[b][2o + q] =
+// sum_{i, c} A[b][2i + c] M[2i + c][2o + q] with A = (Re, Im) of the inputs
+// (BF16 high parts and remainders, two products) and M the real 64 x 64 form
+// of R or of conj(R)^T, whose entries are the exact BF16 weights:
+//   forward: M[2i][2o] = Rr, M[2i+1][2o] = -Ri, M[2i][2o+1] = Ri, M[2i+1][2o+1] = Rr  (of R[i][o])
+//   adjoint: M[2o][2i] = Rr, M[2o+1][2i] = Ri, M[2o][2i+1] = -Ri, M[2o+1][2i+1] = Rr
+// (M's rows indexed by the step's input channel, its columns by the output).
+// The accumulator pair of columns 2t, 2t + 1 is one output's (Re, Im).
+__device__ __forceinline__ uint32_t bf16_pair(unsigned short lo, unsigned short hi) { return (uint32_t)lo | ((uint32_t)hi << 16); }
+
+__global__ void __launch_bounds__(128) mix(const float2* __restrict__ in, float2* __restrict__ out,
+                                           const __nv_bfloat16* __restrict__ w, int l, int B, int adjoint) {
+	const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+	const int mtiles = (B + 15) / 16;
+	const unsigned short* Rr = reinterpret_cast<const unsigned short*>(w + off_Rr(l));
+	const unsigned short* Ri = reinterpret_cast<const unsigned short*>(w + off_Ri(l));
+	const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+	// one warp per (n-tile of eight output columns, mode, 16 batch rows); whole
+	// warps take the same items, so the mma.sync lanes stay converged
+	for (long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wid < (long long)NK * mtiles * 8;
+	     wid += nw) {
+		const int nt = (int)(wid & 7), km = (int)((wid >> 3) % NK), mt = (int)((wid >> 3) / NK);
+		const int b0 = 16 * mt + g, b1 = b0 + 8;
+		const int col = 4 * nt + (g >> 1), q = g & 1; // output channel and part of column 8 nt + g
+		float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+		for (int ks = 0; ks < 4; ks++) {
+			const int i0 = 8 * ks + t, i1 = i0 + 4;
+			const float2 zero = make_float2(0.f, 0.f);
+			const float2 z00 = b0 < B ? in[((long long)b0 * C + i0) * NK + km] : zero;
+			const float2 z10 = b1 < B ? in[((long long)b1 * C + i0) * NK + km] : zero;
+			const float2 z01 = b0 < B ? in[((long long)b0 * C + i1) * NK + km] : zero;
+			const float2 z11 = b1 < B ? in[((long long)b1 * C + i1) * NK + km] : zero;
+			uint32_t ah[4], al[4];
+			split2(z00.x, z00.y, ah[0], al[0]);
+			split2(z10.x, z10.y, ah[1], al[1]);
+			split2(z01.x, z01.y, ah[2], al[2]);
+			split2(z11.x, z11.y, ah[3], al[3]);
+			uint32_t bw[2];
+#pragma unroll
+			for (int h = 0; h < 2; h++) {
+				const int row = 8 * ks + t + 4 * h; // input channel of rows 16 ks + 2t (+8 h), + 1
+				const size_t idx = adjoint ? ((size_t)col * C + row) * NK + km : ((size_t)row * C + col) * NK + km;
+				const unsigned short rr = Rr[idx], ri = Ri[idx], nri = ri ^ 0x8000u;
+				if (!adjoint) bw[h] = q ? bf16_pair(ri, rr) : bf16_pair(rr, nri);
+				else bw[h] = q ? bf16_pair(nri, rr) : bf16_pair(rr, ri);
+			}
+			mma_bf16(d, ah, bw);
+			mma_bf16(d, al, bw);
 		}
-		out[t] = make_float2(ar, ai);
+		const int oc = 4 * nt + t;
+		if (b0 < B) out[((long long)b0 * C + oc) * NK + km] = make_float2(d[0], d[1]);
+		if (b1 < B) out[((long long)b1 * C + oc) * NK + km] = make_float2(d[2], d[3]);
 	}
 }
 
@@ -758,7 +899,6 @@ int grid_for(long long n, int block) {
 	return (int)(g > 148 * 16 ? 148 * 16 : (g < 1 ? 1 : g));
 }
 
-int planes_grid(long long nplanes) { return (int)std::min<long long>(nplanes, 148 * 8); }
 
 thread_local std::string g_fno_err;
 
@@ -776,6 +916,8 @@ struct pfcg_fno {
 	float2* tw = nullptr;        // twiddles of the tile size
 	uint4* fdx = nullptr;        // mma fragments of the truncated x transforms (dft_frag_kernel)
 	uint4* fix = nullptr;
+	uint4* fdy = nullptr;        // mma fragments of the truncated y transforms (dfty_frag_kernel)
+	uint4* fiy = nullptr;
 	float* sx = nullptr;         // per-kx weights of the truncated irfft2: (kx ? 2 : 1) / T^2
 	float* v[L + 1] = {};        // layer inputs (v[L] feeds the projection)
 	float* z[L] = {};            // pre-activations
@@ -821,9 +963,9 @@ int forward(pfcg_fno* f, const float* x, int B, const float* target, bool train)
 	f->launches++;
 	for (int l = 0; l < L; l++) {
 		dft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->v[l], f->A, f->fdx, nullptr, rows, T);
-		dft_y<<<planes_grid(planes), 128, 0, st>>>(f->A, f->X[l], f->tw, planes, T, 0);
-		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->w, l, B, 0);
-		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Y, f->Bq, f->tw, planes, T, 1);
+		dft_y_fwd<<<grid_for(planes * 32 * DY_WARPS, 32 * DY_WARPS), 32 * DY_WARPS, 0, st>>>(f->A, f->X[l], f->fdy, planes, T);
+		mix<<<grid_for((long long)NK * ((B + 15) / 16) * 8 * 32, 128), 128, 0, st>>>(f->X[l], f->Y, f->w, l, B, 0);
+		dft_y_inv<<<grid_for(planes * 32 * DY_WARPS, 32 * DY_WARPS), 32 * DY_WARPS, 0, st>>>(f->Y, f->Bq, f->fiy, planes, T);
 		idft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->Bq, f->s, f->fix, f->sx, rows, T, 0);
 		pointwise_fwd<<<grid_for((long long)B * npix / 16 * 32, 128), 128, 0, st>>>(f->v[l], f->s, f->w, l, train ? f->z[l] : nullptr,
 		                                                                    f->v[l + 1], B, npix, l < L - 1);
@@ -855,10 +997,10 @@ int backward(pfcg_fno* f, const float* x, int B) {
 		weight_grad<<<wg, WG_THREADS, 0, st>>>(f->dz, f->v[l], f->g + off_W(l), f->g + off_b(l), B, npix);
 		// spectral branch, in reverse
 		dft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->dz, f->Bq, f->fdx, f->sx, rows, T);
-		dft_y<<<planes_grid(planes), 128, 0, st>>>(f->Bq, f->Y, f->tw, planes, T, 0);
+		dft_y_fwd<<<grid_for(planes * 32 * DY_WARPS, 32 * DY_WARPS), 32 * DY_WARPS, 0, st>>>(f->Bq, f->Y, f->fdy, planes, T);
 		mix_grad<<<grid_for((long long)C * C * NK, 256), 256, 0, st>>>(f->X[l], f->Y, f->g, l, B);
-		mix<<<grid_for(planes * NK, 256), 256, 0, st>>>(f->Y, f->Bq, f->w, l, B, 1);
-		dft_y<<<planes_grid(planes), 256, 0, st>>>(f->Bq, f->A, f->tw, planes, T, 1);
+		mix<<<grid_for((long long)NK * ((B + 15) / 16) * 8 * 32, 128), 128, 0, st>>>(f->Y, f->Bq, f->w, l, B, 1);
+		dft_y_inv<<<grid_for(planes * 32 * DY_WARPS, 32 * DY_WARPS), 32 * DY_WARPS, 0, st>>>(f->Bq, f->A, f->fiy, planes, T);
 		idft_x<<<grid_for(rows * 2, 256), 256, 0, st>>>(f->A, f->dv2, f->fix, nullptr, rows, T, 1);
 		f->launches += 8;
 		std::swap(f->dv, f->dv2);
@@ -947,6 +1089,8 @@ int pfcg_fno_create(int tile, int max_batch, pfcg_fno** out) {
 	add((void**)&f->tw, sizeof(float2) * tile);
 	add((void**)&f->fdx, sizeof(uint4) * (tile / 16) * 2 * 32);
 	add((void**)&f->fix, sizeof(uint4) * (tile / 8) * 32);
+	add((void**)&f->fdy, sizeof(uint4) * (tile / 8) * 32 * 2);
+	add((void**)&f->fiy, sizeof(uint4) * (tile / 16) * 2 * 32 * 2);
 	add((void**)&f->sx, sizeof(float) * MX);
 	for (int l = 0; l <= L; l++) add((void**)&f->v[l], sizeof(float) * nv);
 	for (int l = 0; l < L; l++) add((void**)&f->z[l], sizeof(float) * nv);
@@ -973,6 +1117,7 @@ int pfcg_fno_create(int tile, int max_batch, pfcg_fno** out) {
 	e = cudaMemcpyAsync(f->sx, sc, sizeof(sc), cudaMemcpyHostToDevice, f->stream);
 	twiddle_kernel<<<1, 256, 0, f->stream>>>(f->tw, tile);
 	dft_frag_kernel<<<(tile * 8 + 255) / 256, 256, 0, f->stream>>>(f->tw, tile, f->fdx, f->fix);
+	dfty_frag_kernel<<<(tile * 8 + 255) / 256, 256, 0, f->stream>>>(f->tw, tile, f->fdy, f->fiy);
 	f->launches += 2;
 	for (size_t i = 0; i < 5 && e == cudaSuccess; i++) e = cudaMemsetAsync(*bufs[i], 0, sizes[i], f->stream);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(f->stream);
@@ -988,8 +1133,8 @@ int pfcg_fno_create(int tile, int max_batch, pfcg_fno** out) {
 void pfcg_fno_destroy(pfcg_fno* f) {
 	if (!f) return;
 	if (f->stream) cudaStreamSynchronize(f->stream);
-	void* ptrs[] = {f->p,  f->w,  f->g,   f->am, f->av, f->tw, f->sx,   f->s,         f->A,   f->Y,
-	                f->Bq, f->dv, f->dv2, f->dz, f->x,  f->y,  f->dy, f->loss, f->field_tmp, f->part};
+	void* ptrs[] = {f->p,  f->w,  f->g,  f->am, f->av,   f->tw,        f->sx,   f->s,   f->A,   f->Y,   f->Bq, f->dv,
+	                f->dv2, f->dz, f->x, f->y,  f->dy,   f->loss,      f->field_tmp, f->part, f->fdx, f->fix, f->fdy, f->fiy};
 	for (void* q : ptrs) cudaFree(q);
 	for (int l = 0; l <= L; l++) cudaFree(f->v[l]);
 	for (int l = 0; l < L; l++) {

@@ -1339,7 +1339,10 @@ template <typename K> static int resident_grid(K k, const LaunchCfg& c, int& res
 // next pass's CTAs may be scheduled while the last wave of the previous one
 // drains, and each kernel waits for the previous kernel's completion and
 // memory (griddepcontrol.wait, its first statement) before touching anything
-// that kernel writes. PFCG_PDL=0 launches them plainly.
+// that kernel writes. PFCG_PDL=0 launches them plainly. Persistent grids (one
+// CTA per resident slot, the FP64 specialised kernels) launch plainly too:
+// with every slot taken there is no drain to overlap, and dependent launches
+// measured 2 % slower there (1.041 against 1.019 ms per 4096^2 U=2 FP64 step).
 static bool pdl_on() {
 	static const int on = [] {
 		const char* e = std::getenv("PFCG_PDL");
@@ -1350,7 +1353,7 @@ static bool pdl_on() {
 
 template <typename K, typename A>
 static cudaError_t pdl_launch(K k, int grid, int block, int smem, cudaStream_t s, const A& a, int n) {
-	if (!pdl_on()) {
+	if (!pdl_on() || grid < n) {
 		k<<<grid, block, smem, s>>>(a, n);
 		return cudaGetLastError();
 	}

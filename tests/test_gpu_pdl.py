@@ -1,0 +1,51 @@
+"""The x- and y-pass kernels launched as programmatic dependent launches (the
+default) give the same fields as plain launches (PFCG_PDL=0). The switch is
+read once per process, so each arm runs in its own interpreter.
+
+The comparison allows 1e-12: the FP64 sums of the nonlinear term are added
+across CTAs with atomics, so their order, and the last bits of the mean that
+download() adds to every point, vary from run to run with any launch mode. A
+kernel that read its predecessor's results too early would be off by far more."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+SNIPPET = r"""
+import sys
+import numpy as np
+sys.path.insert(0, {root!r})
+from pfc_b200 import lib, synth
+from pfc_b200 import params as P
+U, N, prec, out = {U}, {N}, {prec!r}, {out!r}
+if U == 1:
+    p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+    f0 = synth.noise_state(N, N, 0.25, 0.05, 3)[None]
+else:
+    p = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
+    f0 = synth.stripes2(N, N, 0.7, 0.7, max(N // 8, 8), (0.3, -0.3), (0.3, 0.3), (7.2552, 7.2552 * 1.04), 0.02, 4)
+with lib.Relaxation(p, N, N, 0.7, 0.7, prec) as r:
+    r.upload(f0)
+    r.step(9)
+    fave, nave = r.evaluate()
+    np.save(out, np.concatenate([r.download().ravel(), [fave], list(nave)]))
+"""
+
+
+@pytest.mark.parametrize("U,N,prec", [(2, 4096, "fp32"), (1, 512, "fp32"), (2, 256, "fp64"), (2, 384, "fp32")])
+def test_dependent_launch_matches_plain_launch(U, N, prec, tmp_path):
+    res = {}
+    for mode in ("1", "0"):
+        out = str(tmp_path / ("pdl%s.npy" % mode))
+        env = dict(os.environ, PFCG_PDL=mode)
+        code = SNIPPET.format(root=ROOT, U=U, N=N, prec=prec, out=out)
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        res[mode] = np.load(out)
+    assert np.all(np.isfinite(res["1"])) and np.abs(res["1"] - res["0"]).max() < 1e-12
