@@ -73,6 +73,7 @@ struct pfcg_handle {
 	double* d_real = nullptr;   // U*Ny*Nx doubles
 	double* d_fields = nullptr; // f(r) work fields
 	double* d_part = nullptr;   // partial sums of the field means
+	double* nlpart = nullptr;   // per-tile sums of the nonlinear term of a step (U per row tile, Ny tiles at most)
 	int regio = 1;              // y-pass register ends (PFCG_YPASS_REGIO=0: load/store phases through shared memory)
 	void* tmap = nullptr;       // device copy of the y-pass's TMA tensor map over `work` (null: plain loads)
 	int tma_tiles = 0;          // row tiles per TMA box
@@ -418,6 +419,7 @@ template <typename T> XArgs<T> xargs(pfcg_handle* h) {
 	a.sb = h->sbx;
 	a.m = h->model;
 	a.g = h->geom;
+	a.part = h->nlpart;
 	return a;
 }
 
@@ -442,6 +444,8 @@ template <typename T> YArgs<T> yargs(pfcg_handle* h) {
 	a.tma_timeout_ns = h->tma_timeout_ns;
 	a.flag = h->flag;
 	a.k = host_step_k<T>(h->model, h->geom);
+	a.part = h->nlpart;
+	a.nparts = h->Ny / h->geom.R;
 	return a;
 }
 
@@ -875,6 +879,7 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	CKC(cudaMalloc(&h->offs, sizeof(double) * OFFS_N));
 	CKC(cudaMalloc(&h->flag, sizeof(int)));
 	CKC(cudaMalloc(&h->d_part, sizeof(double) * MAXU * MEAN_BLOCKS));
+	CKC(cudaMalloc(&h->nlpart, sizeof(double) * MAXU * Ny));
 	CKC(cudaMallocHost(&h->h_flag, sizeof(int)));
 	CKC(cudaMallocHost(&h->h_buf, sizeof(double) * (ACC_N + MAXU + OFFS_N)));
 	CKC(cudaMemset(h->spec, 0, h->celem * nspec * h->U));
@@ -882,6 +887,7 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	CKC(cudaMemset(h->mean, 0, sizeof(double) * MAXU));
 	CKC(cudaMemset(h->acc, 0, sizeof(double) * ACC_N));
 	CKC(cudaMemset(h->flag, 0, sizeof(int)));
+	CKC(cudaMemset(h->nlpart, 0, sizeof(double) * MAXU * Ny));
 #undef CKC
 	rc = fp64 ? upload_twiddles<double>(h, Nx, &h->twx) : upload_twiddles<float>(h, Nx, &h->twx);
 	if (!rc) rc = fp64 ? upload_twiddles<double>(h, Ny, &h->twy) : upload_twiddles<float>(h, Ny, &h->twy);
@@ -915,6 +921,7 @@ void pfcg_destroy(pfcg_handle* h) {
 	cudaFree(h->d_real);
 	cudaFree(h->d_fields);
 	cudaFree(h->d_part);
+	cudaFree(h->nlpart);
 	for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
 	if (h->h_flag) cudaFreeHost(h->h_flag);
 	if (h->h_buf) cudaFreeHost(h->h_buf);
@@ -1615,6 +1622,7 @@ size_t noalloc_bytes(int U, int Nx, int Ny) {
 	       + align256(sizeof(double) * ACC_N)              // accumulators
 	       + align256(sizeof(int))                         // NaN flag
 	       + align256(sizeof(double) * MAXU * MEAN_BLOCKS) // partial sums of the means
+	       + align256(sizeof(double) * MAXU * Ny)          // per-tile sums of the nonlinear term
 	       + align256(sizeof(float2) * Nx) + align256(sizeof(float2) * Ny);
 }
 
@@ -1686,6 +1694,7 @@ extern "C" int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double d
 	h.acc = (double*)carve(sizeof(double) * ACC_N);
 	h.flag = (int*)carve(sizeof(int));
 	h.d_part = (double*)carve(sizeof(double) * MAXU * MEAN_BLOCKS);
+	h.nlpart = (double*)carve(sizeof(double) * MAXU * Ny);
 	h.twx = carve(sizeof(float2) * Nx);
 	h.twy = carve(sizeof(float2) * Ny);
 	h.d_real = fields; // the caller's buffer is both input and output
@@ -1693,7 +1702,7 @@ extern "C" int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double d
 	auto done = [&](int code) {
 		// the handle's pointers are views of the static workspace: nothing to free
 		h.spec = h.work = h.twx = h.twy = nullptr;
-		h.mean = h.acc = h.d_part = nullptr;
+		h.mean = h.acc = h.d_part = h.nlpart = nullptr;
 		h.flag = nullptr;
 		h.d_real = nullptr;
 		return code ? fail(nullptr, code, h.err) : 0;

@@ -97,6 +97,10 @@ template <typename T> struct XArgs {
 	int sb;                 // channel pairs per FFT call
 	Model m;
 	Geom g;
+	// STEP: the block sums of the nonlinear term go to part[tile * U + u] (the
+	// y-pass adds them in a fixed order, so a step is bit-reproducible);
+	// nullptr: atomically into acc
+	double* part;
 };
 
 // Parameters of one k-space weight (YP_WEIGHT), resolved on the host so the
@@ -138,6 +142,8 @@ template <typename T> struct YArgs {
 	unsigned long long tma_timeout_ns; // bound of that wait
 	int* flag;              // bit 1: a bounded device wait ran out (PFCG_ETIMEOUT)
 	StepK<T> k;             // STEP: the update's constants
+	const double* part;     // STEP: the x-pass's per-tile sums of the nonlinear term (nullptr: acc)
+	int nparts;             //   and their number of tiles
 };
 
 // Flag bits of the step kernels' status word

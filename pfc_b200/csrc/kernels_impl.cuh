@@ -46,7 +46,11 @@ constexpr int MAXNT = 512; // threads per CTA of the FFT kernels
 
 // --------------------------------------------------------------- helpers --
 
-template <int NV> __device__ __forceinline__ void block_reduce_add(double (&v)[NV], double* dst) {
+// The block's sums of v: with store, written to dst (one CTA per slot, so the
+// result does not depend on the order CTAs finish in); otherwise added
+// atomically. Both trees are fixed: shuffles within each warp, then warp 0 over
+// the warps in order.
+template <int NV> __device__ __forceinline__ void block_reduce_put(double (&v)[NV], double* dst, bool store) {
 	__shared__ double red[32][NV > 0 ? NV : 1];
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int nw = (blockDim.x + 31) >> 5;
@@ -64,9 +68,16 @@ template <int NV> __device__ __forceinline__ void block_reduce_add(double (&v)[N
 			double x = lane < nw ? red[lane][i] : 0.0;
 #pragma unroll
 			for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-			if (lane == 0) atomicAdd(dst + i, x);
+			if (lane == 0) {
+				if (store) dst[i] = x;
+				else atomicAdd(dst + i, x);
+			}
 		}
 	}
+}
+
+template <int NV> __device__ __forceinline__ void block_reduce_add(double (&v)[NV], double* dst) {
+	block_reduce_put<NV>(v, dst, false);
 }
 
 template <typename T> __device__ __forceinline__ T expT(T x);
@@ -243,13 +254,42 @@ template <typename T, int U, int N> __device__ __forceinline__ T pick(const T (&
 	return r;
 }
 
-// k = 0 in FP64 (one thread): mean' = A(0) mean + B(0) (sum NL + couplings),
-// pfc-relax.c:1215-1244 at k = 0; clears the NL sums for the next step
-template <typename T, int U> __device__ __forceinline__ void ypass_mean_update(const YArgs<T>& a) {
+// k = 0 in FP64: mean' = A(0) mean + B(0) (sum NL + couplings),
+// pfc-relax.c:1215-1244 at k = 0. The sum of the nonlinear term is that of the
+// x-pass's per-tile sums, added by the whole CTA in a fixed order (thread t
+// takes tiles t, t + nt, ..., then a fixed tree), or the atomically summed
+// accumulator, which is cleared for the next step. Called by every thread of
+// the CTA that holds column kx = 0.
+template <typename T, int U> __device__ __forceinline__ void ypass_mean_update(const YArgs<T>& a, int tid, int nt) {
+	__shared__ double red[32][U];
+	double s[U];
+#pragma unroll
+	for (int u = 0; u < U; u++) s[u] = 0.0;
+	if (a.part) {
+		for (int i = tid; i < a.nparts; i += nt)
+#pragma unroll
+			for (int u = 0; u < U; u++) s[u] += a.part[(long long)i * U + u];
+		const int lane = tid & 31, warp = tid >> 5, nwp = (nt + 31) >> 5;
+#pragma unroll
+		for (int u = 0; u < U; u++)
+#pragma unroll
+			for (int o = 16; o; o >>= 1) s[u] += __shfl_down_sync(0xffffffffu, s[u], o);
+		if (lane == 0)
+#pragma unroll
+			for (int u = 0; u < U; u++) red[warp][u] = s[u];
+		__syncthreads();
+		if (tid == 0)
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				s[u] = 0.0;
+				for (int w = 0; w < nwp; w++) s[u] += red[w][u];
+			}
+	}
+	if (tid != 0) return;
 	const double NxNy = (double)a.g.Nx * (double)a.g.Ny;
 	double mean0[U], Mk[U];
 #pragma unroll
-	for (int u = 0; u < U; u++) { mean0[u] = a.mean[u]; Mk[u] = a.acc[u]; }
+	for (int u = 0; u < U; u++) { mean0[u] = a.mean[u]; Mk[u] = a.part ? s[u] : a.acc[u]; }
 #pragma unroll
 	for (int u = 0; u < U - 1; u++)
 #pragma unroll
@@ -273,7 +313,7 @@ template <typename T, int U> __device__ __forceinline__ void ypass_mean_update(c
 			B = ((av == 0.0) ? o * a.m.dt : (A - 1.0) / av) / NxNy;
 		}
 		a.mean[u] = A * mean0[u] + B * Mk[u];
-		a.acc[u] = 0.0;
+		if (!a.part) a.acc[u] = 0.0;
 	}
 }
 
@@ -415,7 +455,7 @@ __device__ __forceinline__ void xpass_step_fused(const XArgs<T>& a, cplx<T>* sm,
 	double acc[U];
 #pragma unroll
 	for (int u = 0; u < U; u++) acc[u] = (double)accT[u];
-	block_reduce_add<U>(acc, a.acc);
+	block_reduce_put<U>(acc, a.part ? a.part + (long long)tile * U : a.acc, a.part != nullptr);
 }
 
 // y-pass STEP: Z columns from global straight into the first forward pass ->
@@ -547,7 +587,7 @@ __device__ __forceinline__ void ypass_step_fused(const YArgs<T>& a, cplx<T>* sm,
 			dst[(long long)(y / RC) * tileH + y % RC] = rb.v[0][r];
 		}
 	}
-	if (kx0 == 0 && tid == 0) ypass_mean_update<T, U>(a);
+	if (kx0 == 0) ypass_mean_update<T, U>(a, tid, NT);
 }
 
 // ----------------------------------------------------------------- x-pass --
@@ -714,7 +754,7 @@ __device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile, co
 		}
 		if constexpr (MODE == XP_STEP) {
 			if (nan) atomicOr(a.flag, 1);
-			block_reduce_add<NACC>(acc, a.acc);
+			block_reduce_put<NACC>(acc, a.part ? a.part + (long long)tile * U : a.acc, a.part != nullptr);
 		} else if constexpr (MODE == XP_EVAL) {
 			block_reduce_add<NACC>(acc, a.acc);
 		}
@@ -1067,7 +1107,7 @@ __device__ __forceinline__ void ypass_body(const YArgs<T>& a, const int grp, con
 				update(c, kx, ky, Nv);
 			}
 		}
-		if (kx0 == 0 && tid == 0) ypass_mean_update<T, U>(a);
+		if (kx0 == 0) ypass_mean_update<T, U>(a, tid, nt);
 	} else if constexpr (MODE == YP_INIT) {
 		const T invN = (T)(1.0 / ((double)Nx * (double)Ny));
 		for (int e = tid; e < CC * Ny; e += nt) {

@@ -1,6 +1,5 @@
-"""The y-pass's TMA column loads: the same fields as the plain loads
-(PFCG_TMA=0; to 1e-12, since only the order of the atomically summed FP64
-means may differ), and the bounded mbarrier wait, made to run out on purpose
+"""The y-pass's TMA column loads: the same fields bit for bit as the plain
+loads (PFCG_TMA=0), and the bounded mbarrier wait, made to run out on purpose
 with the test hook PFCG_TMA_TEST_STALL (the wait then expects more bytes than
 the loads bring, gives up after 1 ms and the step returns PFCG_ETIMEOUT; the
 loads themselves are unchanged), after which a fresh handle steps normally."""
@@ -32,9 +31,7 @@ def test_tma_loads_match_plain_loads(U, N, monkeypatch):
             r.upload(f0)
             r.step(7)
             out[mode] = r.download()
-    # the FP64 mean that download() adds comes from sums accumulated with
-    # atomics (order-dependent in the last bits), hence 1e-12 and not equality
-    assert np.abs(out["1"] - out["0"]).max() < 1e-12
+    assert np.array_equal(out["1"], out["0"])
 
 
 def test_tma_wait_times_out_on_purpose(monkeypatch):
