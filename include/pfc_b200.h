@@ -189,7 +189,9 @@ int pfcg_get_time(const pfcg_handle* h, int* t);
 
 /* Advances nsteps semi-implicit (ETD1) steps. Replaces step() (:1134-1248)
  * called nsteps times. Returns 39 if a NaN appeared in the field (the
- * reference checks m[0][0] at :1176; this checks every point). */
+ * reference checks m[0][0] at :1176; this checks every point). Steps, like
+ * pfcg_evaluate and pfcg_optimize, are bit-reproducible for a given library
+ * build and device: every sum over CTAs is added in a fixed order. */
 int pfcg_step(pfcg_handle* h, int nsteps);
 
 /* Computes <f> and <n_u> of the current state, and the free-energy density f(r)

@@ -38,6 +38,11 @@ constexpr int ACC_TRIAL = 16; // MAX_TRIAL doubles: Parseval sums per box size
 constexpr int ACC_N = 24;
 constexpr int OFFS_N = 32;    // per-field offsets for the f(r) fields
 constexpr int MAX_THREADS = 512;
+// doubles of a handle's block-sum slots: a step's U per row tile, evaluate's
+// 1 + U per row tile (Ny tiles at most) or its MAX_TRIAL per Parseval block
+size_t nlpart_elems(int Ny) {
+	return std::max((size_t)(MAXU + 1) * Ny, (size_t)MAX_TRIAL * KSPACE_MAX_BLOCKS);
+}
 constexpr double PI = 3.14159265358979323846264338327;
 
 thread_local std::string g_err;
@@ -73,7 +78,8 @@ struct pfcg_handle {
 	double* d_real = nullptr;   // U*Ny*Nx doubles
 	double* d_fields = nullptr; // f(r) work fields
 	double* d_part = nullptr;   // partial sums of the field means
-	double* nlpart = nullptr;   // per-tile sums of the nonlinear term of a step (U per row tile, Ny tiles at most)
+	double* nlpart = nullptr;   // per-block sums added in a fixed order: of the nonlinear term in a step (U per
+	                            // row tile), of evaluate's local terms (1 + U per tile) and Parseval sums
 	int regio = 1;              // y-pass register ends (PFCG_YPASS_REGIO=0: load/store phases through shared memory)
 	void* tmap = nullptr;       // device copy of the y-pass's TMA tensor map over `work` (null: plain loads)
 	int tma_tiles = 0;          // row tiles per TMA box
@@ -591,11 +597,14 @@ template <typename T> int eval_sums(pfcg_handle* h, int ntrial, const double* dx
 		xa.acc = h->acc + ACC_EVAL;
 		int rc = run_xpass<T>(h, XP_EVAL, xa, h->cx);
 		if (rc) return rc;
+		// the row tiles' sums, added in a fixed order
+		CK(h, launch_sum_parts(h->nlpart, h->cx.grid, 1 + h->U, h->acc + ACC_EVAL, h->stream));
+		h->launches++;
 	}
-	h->launches++;
+	h->launches += 2;
 	ProfScope ps(h, 2);
 	CK(h, launch_kspace_energy<T>((const cplx<T>*)h->spec, (long long)h->H * h->Ny, h->model, h->geom, ntrial, dxs, dys,
-	                              h->acc + ACC_TRIAL, h->stream));
+	                              h->acc + ACC_TRIAL, h->nlpart, h->stream));
 	CK(h, cudaMemcpyAsync(h->h_buf, h->acc, sizeof(double) * ACC_N, cudaMemcpyDeviceToHost, h->stream));
 	CK(h, cudaMemcpyAsync(h->h_buf + ACC_N, h->mean, sizeof(double) * h->U, cudaMemcpyDeviceToHost, h->stream));
 	CK(h, cudaStreamSynchronize(h->stream));
@@ -879,7 +888,7 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	CKC(cudaMalloc(&h->offs, sizeof(double) * OFFS_N));
 	CKC(cudaMalloc(&h->flag, sizeof(int)));
 	CKC(cudaMalloc(&h->d_part, sizeof(double) * MAXU * MEAN_BLOCKS));
-	CKC(cudaMalloc(&h->nlpart, sizeof(double) * MAXU * Ny));
+	CKC(cudaMalloc(&h->nlpart, sizeof(double) * nlpart_elems(Ny)));
 	CKC(cudaMallocHost(&h->h_flag, sizeof(int)));
 	CKC(cudaMallocHost(&h->h_buf, sizeof(double) * (ACC_N + MAXU + OFFS_N)));
 	CKC(cudaMemset(h->spec, 0, h->celem * nspec * h->U));
@@ -887,7 +896,7 @@ int pfcg_create(const pfcg_params* p, int Nx, int Ny, double dx, double dy, pfcg
 	CKC(cudaMemset(h->mean, 0, sizeof(double) * MAXU));
 	CKC(cudaMemset(h->acc, 0, sizeof(double) * ACC_N));
 	CKC(cudaMemset(h->flag, 0, sizeof(int)));
-	CKC(cudaMemset(h->nlpart, 0, sizeof(double) * MAXU * Ny));
+	CKC(cudaMemset(h->nlpart, 0, sizeof(double) * nlpart_elems(Ny)));
 #undef CKC
 	rc = fp64 ? upload_twiddles<double>(h, Nx, &h->twx) : upload_twiddles<float>(h, Nx, &h->twx);
 	if (!rc) rc = fp64 ? upload_twiddles<double>(h, Ny, &h->twy) : upload_twiddles<float>(h, Ny, &h->twy);

@@ -98,7 +98,8 @@ template <typename T> struct XArgs {
 	Model m;
 	Geom g;
 	// STEP: the block sums of the nonlinear term go to part[tile * U + u] (the
-	// y-pass adds them in a fixed order, so a step is bit-reproducible);
+	// y-pass adds them in a fixed order, so a step is bit-reproducible); EVAL:
+	// the 1 + U sums to part[tile * (1 + U) + i] (added by launch_sum_parts);
 	// nullptr: atomically into acc
 	double* part;
 };
@@ -187,10 +188,16 @@ template <typename T>
 cudaError_t launch_generic_batch(int pass, const void* probs, const int* bp, const int* bl, int nblk, int threads,
                                  int smem, cudaStream_t s);
 
-// Parseval sums for up to MAX_TRIAL box sizes (see kernels.cu): out[t] += ...
+// Parseval sums for up to MAX_TRIAL box sizes: out[t] = ... With part
+// (MAX_TRIAL * KSPACE_MAX_BLOCKS doubles) the blocks' sums are added in a fixed
+// order; without it they are added to out atomically.
+constexpr int KSPACE_MAX_BLOCKS = 148 * 8;
 template <typename T>
 cudaError_t launch_kspace_energy(const cplx<T>* spec, long long sstride, const Model& m, const Geom& g, int ntrial,
-                                 const double* dxs, const double* dys, double* out, cudaStream_t s);
+                                 const double* dxs, const double* dys, double* out, double* part, cudaStream_t s);
+
+// out[i] = sum over p < nparts of part[p * nv + i] in a fixed order (i < nv)
+cudaError_t launch_sum_parts(const double* part, int nparts, int nv, double* out, cudaStream_t s);
 
 // Deterministic FP64 means of U real fields (npts each): per-block partial
 // sums into part[U * nblocks], then one block per field adds them in order.

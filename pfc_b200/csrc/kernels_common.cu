@@ -161,6 +161,27 @@ __global__ void __launch_bounds__(256) finish_means_kernel(const double* __restr
 	if (threadIdx.x == 0) mean[u] = red[0] / (double)npts;
 }
 
+// out[i] = sum over p of part[p * nv + i], p in a fixed order (one block per i)
+__global__ void __launch_bounds__(256) sum_parts_kernel(const double* __restrict__ part, int nparts, int nv,
+                                                         double* __restrict__ out) {
+	const int i = blockIdx.x;
+	double s = 0.0;
+	for (int p = threadIdx.x; p < nparts; p += 256) s += part[(long long)p * nv + i];
+	__shared__ double red[256];
+	red[threadIdx.x] = s;
+	__syncthreads();
+	for (int o = 128; o; o >>= 1) {
+		if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) out[i] = red[0];
+}
+
+cudaError_t launch_sum_parts(const double* part, int nparts, int nv, double* out, cudaStream_t s) {
+	sum_parts_kernel<<<nv, 256, 0, s>>>(part, nparts, nv, out);
+	return cudaGetLastError();
+}
+
 cudaError_t launch_field_means(const double* real, int U, long long npts, double* part, int nblocks, double* mean,
                                cudaStream_t s) {
 	partial_sums_kernel<<<dim3(nblocks, U), 256, 0, s>>>(real, npts, part);

@@ -6,7 +6,7 @@ namespace pfcg {
 template cudaError_t launch_xpass<float>(int, const XArgs<float>&, const LaunchCfg&, cudaStream_t);
 template cudaError_t launch_ypass<float>(int, const YArgs<float>&, const LaunchCfg&, cudaStream_t);
 template cudaError_t launch_kspace_energy<float>(const cplx<float>*, long long, const Model&, const Geom&, int, const double*,
-                                               const double*, double*, cudaStream_t);
+                                               const double*, double*, double*, cudaStream_t);
 
 template cudaError_t launch_ct_batch<float>(int, int, int, const void*, const int*, const int*, int, const LaunchCfg&,
                                            cudaStream_t);

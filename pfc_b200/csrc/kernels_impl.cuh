@@ -756,7 +756,7 @@ __device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile, co
 			if (nan) atomicOr(a.flag, 1);
 			block_reduce_put<NACC>(acc, a.part ? a.part + (long long)tile * U : a.acc, a.part != nullptr);
 		} else if constexpr (MODE == XP_EVAL) {
-			block_reduce_add<NACC>(acc, a.acc);
+			block_reduce_put<NACC>(acc, a.part ? a.part + (long long)tile * NACC : a.acc, a.part != nullptr);
 		}
 	}
 
@@ -1238,7 +1238,8 @@ struct Trials {
 
 template <typename T, int U>
 __global__ void __launch_bounds__(256) kspace_energy_kernel(const cplx<T>* __restrict__ spec, long long sstride, const Model m,
-                                                           const Geom g, int ntrial, const Trials tr, double* out) {
+                                                           const Geom g, int ntrial, const Trials tr, double* out,
+                                                           double* part) {
 	double acc[MAX_TRIAL];
 #pragma unroll
 	for (int t = 0; t < MAX_TRIAL; t++) acc[t] = 0.0;
@@ -1275,7 +1276,7 @@ __global__ void __launch_bounds__(256) kspace_energy_kernel(const cplx<T>* __res
 			}
 		}
 	}
-	block_reduce_add<MAX_TRIAL>(acc, out);
+	block_reduce_put<MAX_TRIAL>(acc, part ? part + (long long)blockIdx.x * MAX_TRIAL : out, part != nullptr);
 }
 
 // -------------------------------------------------------------- launchers --
@@ -1685,7 +1686,7 @@ template <typename T> void prepare_batch_kernels() {
 
 template <typename T>
 cudaError_t launch_kspace_energy(const cplx<T>* spec, long long sstride, const Model& m, const Geom& g, int ntrial,
-                                 const double* dxs, const double* dys, double* out, cudaStream_t s) {
+                                 const double* dxs, const double* dys, double* out, double* part, cudaStream_t s) {
 	Trials tr;
 	for (int t = 0; t < MAX_TRIAL; t++) {
 		tr.dx[t] = t < ntrial ? dxs[t] : 1.0;
@@ -1693,15 +1694,17 @@ cudaError_t launch_kspace_energy(const cplx<T>* spec, long long sstride, const M
 	}
 	const long long total = (long long)g.H * g.Ny;
 	int grid = (int)((total + 255) / 256);
-	if (grid > 148 * 8) grid = 148 * 8;
+	if (grid > KSPACE_MAX_BLOCKS) grid = KSPACE_MAX_BLOCKS;
 	switch (m.U) {
-	case 1: kspace_energy_kernel<T, 1><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
-	case 2: kspace_energy_kernel<T, 2><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
-	case 3: kspace_energy_kernel<T, 3><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
-	case 4: kspace_energy_kernel<T, 4><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out); break;
+	case 1: kspace_energy_kernel<T, 1><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out, part); break;
+	case 2: kspace_energy_kernel<T, 2><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out, part); break;
+	case 3: kspace_energy_kernel<T, 3><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out, part); break;
+	case 4: kspace_energy_kernel<T, 4><<<grid, 256, 0, s>>>(spec, sstride, m, g, ntrial, tr, out, part); break;
 	default: return cudaErrorInvalidValue;
 	}
-	return cudaGetLastError();
+	cudaError_t e = cudaGetLastError();
+	if (e != cudaSuccess || !part) return e;
+	return launch_sum_parts(part, grid, MAX_TRIAL, out, s);
 }
 
 

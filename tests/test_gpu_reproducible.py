@@ -1,9 +1,11 @@
-"""A relaxation step is bit-reproducible: the x-pass writes each row tile's
-sums of the nonlinear term to its own slot and the y-pass adds the slots in a
-fixed order, so repeated runs from the same state give the same fields bit for
-bit (the reference, a serial CPU code, is reproducible the same way). Checked
-for the compile-time specialised kernels (FP32 4096^2 and 512^2, FP64 2048^2),
-the runtime-plan kernels (320^2) and the batch."""
+"""Relaxation steps and energy evaluations are bit-reproducible: the x-pass
+writes each row tile's sums of the nonlinear term to its own slot and the
+y-pass adds the slots in a fixed order, and evaluate() adds its row tiles' and
+Parseval blocks' sums the same way, so repeated runs from the same state give
+the same fields, energies and optimised box bit for bit (the reference, a
+serial CPU code, is reproducible the same way). Checked for the compile-time
+specialised kernels (FP32 4096^2 and 512^2, FP64 2048^2), the runtime-plan
+kernels (320^2) and the batch."""
 import math
 
 import numpy as np
@@ -26,13 +28,18 @@ def _case(U, N):
 @pytest.mark.parametrize("U,N,prec", [(2, 4096, "fp32"), (1, 512, "fp32"), (2, 2048, "fp64"), (1, 320, "fp32")])
 def test_repeated_runs_are_identical(U, N, prec):
     p, d, f0 = _case(U, N)
-    out = []
+    out, en = [], []
     for _ in range(2):
         with lib.Relaxation(p, N, N, d, d, prec) as r:
             r.upload(f0)
             r.step(25)
+            fave, nave = r.evaluate()
+            dd = r.optimize(1, 1, 1e-4)
+            r.step(5)
             out.append(r.download())
+            en.append([fave] + list(nave) + [dd] + list(r.box()))
     assert np.all(np.isfinite(out[0])) and np.array_equal(out[0], out[1])
+    assert en[0] == en[1]
 
 
 def test_repeated_batches_are_identical():
