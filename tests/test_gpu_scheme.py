@@ -112,3 +112,37 @@ def test_scheme_argument_checked():
     with lib.Relaxation(p, 32, 32, 0.7, 0.7, "fp64") as r:
         assert r.scheme == "etd1"
         assert r.L.pfcg_set_scheme(r.h, 7) == lib.EARG
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-6)])
+def test_semi_implicit_in_a_batch(precision, tol):
+    """Problems of one batch on different schemes (set on the problems' handles
+    after the batch was built, so the batch re-uploads their arguments) step
+    like single handles on the same schemes."""
+    p1 = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
+    p2 = P.make_params(P.hetero_2c(0.04), 1.0, 0.25)
+    probs = []
+    for k, (N, U) in enumerate([(256, 1), (384, 2), (96, 2), (256, 1)]):
+        if U == 1:
+            probs.append((p1, N, N, math.pi / 4, math.pi / 4, synth.noise_state(N, N, 0.25, 0.05, 70 + k)[None]))
+        else:
+            probs.append((p2, N, N, 0.7, 0.7, synth.stripes2(N, N, 0.7, 0.7, 16, (0.3, -0.3), (0.3, 0.3),
+                                                             (7.2552, 7.2552 * 1.04), 0.02, 80 + k)))
+    schemes = ["semi", "semi", "etd1", "etd1"]
+    with lib.Batch([q[:5] for q in probs], precision, autotune=False) as b:
+        for prob, q, s in zip(b.problems, probs, schemes):
+            prob.upload(q[5])
+            prob.set_scheme(s)
+        b.step(12)
+        got = [prob.download() for prob in b.problems]
+    for q, s, g in zip(probs, schemes, got):
+        with lib.Relaxation(*q[:5], precision, scheme=s) as r:
+            r.upload(q[5])
+            r.step(12)
+            ref = r.download()
+        assert np.abs(g - ref).max() < tol, s
+    # the two schemes really differ on these states
+    with lib.Relaxation(*probs[0][:5], precision) as r:
+        r.upload(probs[0][5])
+        r.step(12)
+        assert np.abs(r.download() - got[0]).max() > 100 * tol
