@@ -91,6 +91,13 @@ struct pfcg_handle {
 	long long launches = 0;
 	// per-kernel timing (pfcg_set_profiling)
 	bool profiling = false;
+	// STEP_GRAPH steps captured as one CUDA graph and replayed by do_steps, for
+	// the arguments in sgraph_key (recaptured when the box, scheme or launch
+	// shapes change); stepped_plain: a step has run outside capture (the
+	// kernels' attributes are set)
+	cudaGraphExec_t sgraph = nullptr;
+	std::vector<unsigned char> sgraph_key;
+	bool stepped_plain = false;
 	std::vector<cudaEvent_t> ev;     // event pairs, recorded around launches
 	std::vector<int> ev_kind;
 	double prof_ms[3] = {0, 0, 0};
@@ -567,6 +574,43 @@ template <typename T> int do_download(pfcg_handle* h, double* fields, cudaMemcpy
 	return 0;
 }
 
+// Steps per captured step graph. A short step is launch-bound (512^2: two
+// kernels of about 5 us each), and one graph launch for 2 * STEP_GRAPH
+// kernels removes most of the per-launch cost; PFCG_STEP_GRAPH=0 launches
+// every kernel from the host.
+constexpr int STEP_GRAPH = 16;
+
+bool step_graphs_on() {
+	static const int on = [] {
+		const char* e = std::getenv("PFCG_STEP_GRAPH");
+		return (e && e[0] == '0') ? 0 : 1;
+	}();
+	return on != 0;
+}
+
+// Captures STEP_GRAPH steps with these arguments into h->sgraph; on any
+// failure leaves h->sgraph empty, so that the caller launches the steps itself.
+template <typename T> void capture_steps(pfcg_handle* h, const XArgs<T>& xa, const YArgs<T>& ya,
+                                         const std::vector<unsigned char>& key) {
+	if (h->sgraph) cudaGraphExecDestroy(h->sgraph);
+	h->sgraph = nullptr;
+	h->sgraph_key.clear();
+	if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+		cudaGetLastError();
+		return;
+	}
+	bool ok = true;
+	for (int i = 0; i < STEP_GRAPH && ok; i++)
+		ok = launch_xpass<T>(XP_STEP, xa, h->cxs, h->stream) == cudaSuccess &&
+		     launch_ypass<T>(YP_STEP, ya, h->cys, h->stream) == cudaSuccess;
+	cudaGraph_t g = nullptr;
+	const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+	if (ok && e == cudaSuccess && g && cudaGraphInstantiate(&h->sgraph, g, 0) == cudaSuccess) h->sgraph_key = key;
+	else h->sgraph = nullptr;
+	if (g) cudaGraphDestroy(g);
+	cudaGetLastError();
+}
+
 template <typename T> int do_steps(pfcg_handle* h, int nsteps) {
 	XArgs<T> xa = xargs<T>(h);
 	xa.acc = h->acc + ACC_NL;
@@ -574,12 +618,37 @@ template <typename T> int do_steps(pfcg_handle* h, int nsteps) {
 	// The reference resynchronises the spectral state every 100 steps and after
 	// evaluate (pfc-relax.c:1179-1185, 1125-1130); the y-pass does the same
 	// projection every step, so no separate pass is needed.
-	for (int s = 0; s < nsteps; s++) {
+	int s = 0;
+	if (step_graphs_on() && !h->profiling && nsteps >= STEP_GRAPH) {
+		if (!h->stepped_plain) {
+			// the first step of a handle runs plainly (it sets the kernels' attributes)
+			int rc = run_xpass<T>(h, XP_STEP, xa, h->cxs);
+			if (!rc) rc = run_ypass<T>(h, YP_STEP, ya, h->cys);
+			if (rc) return rc;
+			h->t++;
+			s = 1;
+			h->stepped_plain = true;
+		}
+		std::vector<unsigned char> key(sizeof xa + sizeof ya + 2 * sizeof(LaunchCfg));
+		std::memcpy(key.data(), &xa, sizeof xa);
+		std::memcpy(key.data() + sizeof xa, &ya, sizeof ya);
+		std::memcpy(key.data() + sizeof xa + sizeof ya, &h->cxs, sizeof(LaunchCfg));
+		std::memcpy(key.data() + sizeof xa + sizeof ya + sizeof(LaunchCfg), &h->cys, sizeof(LaunchCfg));
+		if (!h->sgraph || key != h->sgraph_key) capture_steps<T>(h, xa, ya, key);
+		if (h->sgraph)
+			for (; s + STEP_GRAPH <= nsteps; s += STEP_GRAPH) {
+				CK(h, cudaGraphLaunch(h->sgraph, h->stream));
+				h->launches += 2 * STEP_GRAPH;
+				h->t += STEP_GRAPH;
+			}
+	}
+	for (; s < nsteps; s++) {
 		int rc = run_xpass<T>(h, XP_STEP, xa, h->cxs);
 		if (rc) return rc;
 		rc = run_ypass<T>(h, YP_STEP, ya, h->cys);
 		if (rc) return rc;
 		h->t++;
+		h->stepped_plain = true;
 	}
 	CK(h, cudaMemcpyAsync(h->h_flag, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
 	CK(h, cudaStreamSynchronize(h->stream));
@@ -934,6 +1003,7 @@ void pfcg_destroy(pfcg_handle* h) {
 	for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
 	if (h->h_flag) cudaFreeHost(h->h_flag);
 	if (h->h_buf) cudaFreeHost(h->h_buf);
+	if (h->sgraph) cudaGraphExecDestroy(h->sgraph);
 	if (h->stream) cudaStreamDestroy(h->stream);
 	delete h;
 }
