@@ -1,4 +1,5 @@
-// Kernel interfaces of the B200 relaxation path (implemented in kernels.cu).
+// Kernel interfaces of the B200 relaxation path (implemented in kernels_impl.cuh,
+// instantiated by kernels_f32*.cu and kernels_f64.cu, and in kernels_common.cu).
 //
 // Data layout in HBM for a system of U fields on an Nx x Ny grid, H = Nx/2+1:
 //
@@ -89,7 +90,7 @@ template <typename T> struct XArgs {
 	long long wstride;
 	const double* off;      // per-field value added after c2r / subtracted before r2c (the mean)
 	double* real;           // XP_C2R output / XP_R2C input: U fields of Ny*Nx doubles
-	double* acc;            // FP64 accumulators (see kernels.cu)
+	double* acc;            // FP64 accumulators of the modes that add atomically (see part)
 	int* flag;              // NaN flag
 	const cplx<T>* tw;      // twiddles of length Nx
 	const cplx<T>* twct;    // per-pass twiddle table of the specialised kernels
@@ -123,7 +124,7 @@ template <typename T> struct YArgs {
 	cplx<T>* spec;          // U arrays at stride sstride
 	long long sstride;
 	double* mean;           // U, updated in place by YP_STEP at k = 0
-	double* acc;            // FP64 sum of NL per field (read and cleared by YP_STEP)
+	double* acc;            // without part: FP64 sum of NL per field (read and cleared by YP_STEP)
 	const cplx<T>* tw;      // twiddles of length Ny
 	const cplx<T>* twct;    // per-pass twiddle table of the specialised kernels
 	FftPlan plan;
@@ -205,7 +206,7 @@ cudaError_t launch_field_means(const double* real, int U, long long npts, double
                                cudaStream_t s);
 
 // f(r) assembly for write_energy: f = sum of local terms of m plus gradient /
-// smoothing couplings from the precomputed real fields (see kernels.cu).
+// smoothing couplings from the precomputed real fields (kernels_common.cu).
 cudaError_t launch_energy_density(const double* m, const double* pn, const double* eta, const double* q, int npair,
                                   const Model& mod, long long npts, double* f, cudaStream_t s);
 
