@@ -2,8 +2,9 @@
 and y-pass kernels as programmatic dependent launches (the default) against
 plain launches (PFCG_PDL=0), and runs of 16 steps replayed as one captured CUDA
 graph (the default) against every kernel launched from the host
-(PFCG_STEP_GRAPH=0). The switches are read once per process, so each arm runs
-in its own interpreter.
+(PFCG_STEP_GRAPH=0), also across changes of the box and the scheme, which make
+the graph be captured again. The switches are read once per process, so each
+arm runs in its own interpreter.
 
 Steps and evaluate() are bit-reproducible (every sum over CTAs is added in a
 fixed order), so the fields and the energies must be equal."""
@@ -24,7 +25,7 @@ import numpy as np
 sys.path.insert(0, {root!r})
 from pfc_b200 import lib, synth
 from pfc_b200 import params as P
-U, N, prec, out, nsteps = {U}, {N}, {prec!r}, {out!r}, {nsteps}
+U, N, prec, out, nsteps, changes = {U}, {N}, {prec!r}, {out!r}, {nsteps}, {changes}
 if U == 1:
     p = P.make_params(P.honeycomb_1c(-0.25), 1.0, 1.0)
     f0 = synth.noise_state(N, N, 0.25, 0.05, 3)[None]
@@ -34,6 +35,15 @@ else:
 with lib.Relaxation(p, N, N, 0.7, 0.7, prec) as r:
     r.upload(f0)
     r.step(nsteps)
+    if changes:
+        # new arguments: the captured step graph must be recaptured each time
+        r.set_box(0.7 * 1.01, 0.7 * 0.99)
+        r.step(33)
+        r.set_scheme("semi")
+        r.step(20)
+        r.set_scheme("etd1")
+        r.set_box(0.7, 0.7)
+        r.step(17)
     fave, nave = r.evaluate()
     np.savez(out, fields=r.download(), energy=np.array([fave] + list(nave)))
 """
@@ -45,7 +55,7 @@ def test_dependent_launch_matches_plain_launch(U, N, prec, tmp_path):
     for mode in ("1", "0"):
         out = str(tmp_path / ("pdl%s.npz" % mode))
         env = dict(os.environ, PFCG_PDL=mode)
-        code = SNIPPET.format(root=ROOT, U=U, N=N, prec=prec, out=out, nsteps=9)
+        code = SNIPPET.format(root=ROOT, U=U, N=N, prec=prec, out=out, nsteps=9, changes=False)
         r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         res[mode] = np.load(out)
@@ -60,7 +70,7 @@ def test_step_graph_matches_host_launches(U, N, prec, tmp_path):
     for mode in ("1", "0"):
         out = str(tmp_path / ("graph%s.npz" % mode))
         env = dict(os.environ, PFCG_STEP_GRAPH=mode)
-        code = SNIPPET.format(root=ROOT, U=U, N=N, prec=prec, out=out, nsteps=41)
+        code = SNIPPET.format(root=ROOT, U=U, N=N, prec=prec, out=out, nsteps=41, changes=True)
         r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         res[mode] = np.load(out)
