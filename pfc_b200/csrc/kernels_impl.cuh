@@ -594,6 +594,9 @@ __device__ __forceinline__ void ypass_step_fused(const YArgs<T>& a, cplx<T>* sm,
 
 // Body of the x-pass for row tile `tile`; called by xpass_kernel (one problem)
 // and by xpass_batch_kernel (many problems in one launch).
+// (in the fused instantiations the code after the early return is unreachable,
+// which is intended)
+#pragma nv_diag_suppress 128
 template <typename T, int U, int MODE, int NC, int RC>
 __device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile, const bool load_tw = true) {
 	using C = XCfg<T, U, NC, RC>;
@@ -788,6 +791,7 @@ __device__ __forceinline__ void xpass_body(const XArgs<T>& a, const int tile, co
 		}
 	}
 }
+#pragma nv_diag_default 128
 
 // ----------------------------------------------------------------- y-pass --
 
