@@ -139,8 +139,9 @@ typedef struct pfcg_grain {
 } pfcg_grain;
 
 /* The Voronoi step on one field (Ny*Nx doubles, y-major; DEVICE or HOST memory,
- * told apart by cudaPointerGetAttributes), read and written in place: each point takes the grain whose centre is nearest under
- * periodic boundaries (closest(), src/PFCInit.java:68-93) and becomes
+ * told apart by cudaPointerGetAttributes), read and written in place: each
+ * point takes the grain whose centre is nearest under periodic boundaries
+ * (closest(), src/PFCInit.java:68-93) and becomes
  * type * old + nave + amp * OMA(r') + 2 namp (U - 0.5) (:444-458), OMA the
  * one-mode lattice of :46-66. U is java.util.Random's nextDouble, drawn once
  * per non-phantom point in row-major order as the Java loop does; *rng is the
@@ -336,13 +337,14 @@ void pfcg_fno_destroy(pfcg_fno* f);
  * on a B200).
  * The workspace is a file-scope array of PFCG_NOALLOC_SCRATCH_BYTES (32 MiB)
  * that every GPU loading the library holds until exit; grids needing more,
- * about 2 * U * (Nx/2+1) * Ny * 8 bytes plus a few KB, are rejected with
- * PFCG_ESIZE. Every call looks up the array's address on the current device
- * (cudaGetSymbolAddress, which allocates nothing). The first call on a device
- * also sets kernel attributes (cudaFuncSetAttribute); make that first call
- * before any stream capture begins. All calls share the one array and it keeps
- * the last call's contents (the call clears what must start at zero), so calls
- * that overlap on the GPU (other streams, other host threads) race.
+ * about 2 * U * (Nx/2+1) * Ny * 8 bytes plus 32 * Ny bytes and a few KB, are
+ * rejected with PFCG_ESIZE. Every call looks up the array's address on the
+ * current device (cudaGetSymbolAddress, which allocates nothing). The first
+ * call on a device also sets kernel attributes (cudaFuncSetAttribute); make
+ * that first call before any stream capture begins. All calls share the one
+ * array and it keeps the last call's contents (the call clears what must start
+ * at zero), so calls that overlap on the GPU (other streams, other host
+ * threads) race.
  * Returns 0, 39 on NaN, or a negative PFCG_E* code (pfcg_last_error(NULL)). */
 int pfcg_relax_noalloc(const pfcg_params* p, int Nx, int Ny, double dx, double dy, int nsteps, double* fields,
                        void* stream);
