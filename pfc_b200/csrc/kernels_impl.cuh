@@ -76,10 +76,6 @@ template <int NV> __device__ __forceinline__ void block_reduce_put(double (&v)[N
 	}
 }
 
-template <int NV> __device__ __forceinline__ void block_reduce_add(double (&v)[NV], double* dst) {
-	block_reduce_put<NV>(v, dst, false);
-}
-
 template <typename T> __device__ __forceinline__ T expT(T x);
 template <> __device__ __forceinline__ float expT<float>(float x) { return expf(x); }
 template <> __device__ __forceinline__ double expT<double>(double x) { return exp(x); }
